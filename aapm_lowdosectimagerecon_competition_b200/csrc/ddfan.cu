@@ -1,0 +1,531 @@
+// ddfan.cu -- host side of libddfan: plans, launches, the C ABI (include/ddfan.h).
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "ddfan.h"
+#include "ddfan_kernels.cuh"
+#include "ddfan_plan.h"
+
+namespace ddfan {
+
+// ------------------------------------------------------------------ errors
+
+static thread_local std::string g_err;
+
+int set_err(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+const char* last_error() { return g_err.c_str(); }
+
+// ------------------------------------------------------------------ plan
+
+static int pow2_zl(int ZB) {
+  if (ZB >= 8) return 8;
+  if (ZB >= 4) return 4;
+  if (ZB >= 2) return 2;
+  return 1;
+}
+
+template <class T>
+static int dalloc(T** p, size_t n, size_t* bytes) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return set_err(DDFAN_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+  }
+  *bytes += n * sizeof(T);
+  return DDFAN_OK;
+}
+
+void plan_free(Plan* P) {
+  if (!P) return;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(P->device);
+  void* ptrs[] = {P->d_bx, P->d_by, P->d_xd, P->d_yd, P->d_mask, P->d_tb, P->d_lut, P->d_satx,
+                  P->d_saty, P->d_satq, P->d_vg, P->d_fc, P->d_cvd, P->d_tmp, P->d_angs};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  if (prev >= 0) cudaSetDevice(prev);
+  delete P;
+}
+
+// DD3Boundaries (AAPM_script/utilities.cuh:268-287): evaluated in double,
+// stored as float like the reference's float arrays.
+static void boundaries(int n, const float* c, std::vector<double>& out) {
+  const int nb = n + 1;
+  out.assign(nb, 0.0);
+  if (nb >= 3) {
+    for (int i = 0; i < nb; ++i) {
+      double v;
+      if (i == 0) v = 1.5 * c[0] - 0.5 * c[1];
+      else if (i == nb - 1) v = 1.5 * c[i - 1] - 0.5 * c[i - 2];
+      else v = 0.5 * c[i - 1] + 0.5 * c[i];
+      out[i] = (double)(float)v;
+    }
+  } else {
+    out[0] = (double)(float)(c[0] - 0.5);
+    out[1] = (double)(float)(c[0] + 0.5);
+  }
+}
+
+int plan_create(Plan** out, const PlanDesc& d) {
+  *out = nullptr;
+  if (d.DNU < 2 || d.XN < 1 || d.YN < 1 || d.SLN < 1 || d.PNmax < 1 || !d.xds || !d.yds)
+    return set_err(DDFAN_ERR_ARG, "plan: bad sizes (DNU=%d XN=%d YN=%d SLN=%d PNmax=%d) or null geometry",
+                   d.DNU, d.XN, d.YN, d.SLN, d.PNmax);
+  if (!(d.dx > 0.f)) return set_err(DDFAN_ERR_ARG, "plan: dx must be > 0");
+  if (d.sat_mode < SAT_FP32 || d.sat_mode > SAT_FP64) return set_err(DDFAN_ERR_ARG, "plan: sat_mode %d", d.sat_mode);
+  if (d.XN > 1024 || d.YN > 1024 || d.DNU + 1 > 1024)
+    return set_err(DDFAN_ERR_UNSUPPORTED, "plan: lines longer than 1024 cells are not supported");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+    cudaGetLastError();
+    return set_err(DDFAN_ERR_CUDA, "no CUDA device");
+  }
+  if (d.device < 0 || d.device >= ndev) return set_err(DDFAN_ERR_ARG, "device %d of %d", d.device, ndev);
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (cudaSetDevice(d.device) != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "cudaSetDevice(%d)", d.device);
+  std::unique_ptr<Plan, void (*)(Plan*)> P(new Plan(), plan_free);
+  Plan& p = *P;
+  p.device = d.device;
+  p.XN = d.XN; p.YN = d.YN; p.U = d.DNU; p.Z = d.SLN; p.ZB = (d.SLN + 3) / 4;
+  p.PNmax = d.PNmax; p.mode = d.sat_mode; p.ZL = pow2_zl(p.ZB);
+  p.x0 = d.x0; p.y0 = d.y0; p.dx = d.dx; p.detCntIdx = d.detCntIdx;
+  p.ocx = (d.XN - 1.0) * 0.5 - (double)d.imgXCenter / (double)d.dx;
+  p.ocy = (d.YN - 1.0) * 0.5 - (double)d.imgYCenter / (double)d.dx;
+  boundaries(d.DNU, d.xds, p.bx);
+  boundaries(d.DNU, d.yds, p.by);
+  p.xd.assign(d.xds, d.xds + d.DNU);
+  p.yd.assign(d.yds, d.yds + d.DNU);
+  // REF backprojector constants (AAPM_script/MultiSlicesBackGPU.cu:141, :150, :211, :226-227)
+  {
+    const double S2D = std::hypot((double)d.xds[0] - d.x0, (double)d.yds[0] - d.y0);
+    const double ex = (double)d.xds[1] - d.xds[0], ey = (double)d.yds[1] - d.yds[0];
+    const double dbeta = std::atan(std::sqrt(ex * ex + ey * ey) / S2D * 0.5) * 2.0;
+    p.inv_dbeta = 1.0 / dbeta;
+    p.inv_sid = 1.0 / std::sqrt((double)d.x0 * d.x0 + (double)d.y0 * d.y0);
+  }
+  // exact-adjoint bracket table: fan tangent of every boundary, seen from the source
+  {
+    const double sl = std::sqrt((double)d.x0 * d.x0 + (double)d.y0 * d.y0);
+    if (!(sl > 0)) return set_err(DDFAN_ERR_ARG, "source at the rotation centre");
+    p.sh0x = -d.x0 / sl; p.sh0y = -d.y0 / sl;
+    std::vector<double> T(d.DNU + 1);
+    for (int b = 0; b <= d.DNU; ++b) {
+      const double vx = p.bx[b] - d.x0, vy = p.by[b] - d.y0;
+      T[b] = (p.sh0x * vy - p.sh0y * vx) / (p.sh0x * vx + p.sh0y * vy);
+    }
+    p.dirt = T[d.DNU] >= T[0] ? 1.f : -1.f;
+    p.tb.resize(d.DNU + 1);
+    bool mono = true;
+    for (int b = 0; b <= d.DNU; ++b) {
+      p.tb[b] = (float)(p.dirt * T[b]);
+      if (b && !(p.tb[b] > p.tb[b - 1])) mono = false;
+    }
+    p.adj_ok = mono;
+    p.M = 4 * (d.DNU + 1);
+    p.t0 = p.tb[0];
+    const double span = (double)p.tb[d.DNU] - p.tb[0];
+    p.invdt = (float)(p.M / span);
+    p.lut.resize(p.M);
+    int b = 0;
+    for (int m = 0; m < p.M; ++m) {
+      const double tm = p.tb[0] + m * span / p.M;
+      while (b < d.DNU && p.tb[b + 1] <= tm) ++b;
+      p.lut[m] = (uint16_t)std::min(b, d.DNU - 1);
+    }
+  }
+  size_t& B = p.bytes;
+  int rc;
+  const size_t F4 = cell_f4(p.mode);
+  const size_t nimg = (size_t)p.XN * p.YN * p.ZB * F4;
+  const size_t nsino = (size_t)p.PNmax * (p.U + 1) * p.ZB * F4;
+  if ((rc = dalloc(&p.d_bx, p.U + 1, &B)) || (rc = dalloc(&p.d_by, p.U + 1, &B)) ||
+      (rc = dalloc(&p.d_xd, p.U, &B)) || (rc = dalloc(&p.d_yd, p.U, &B)) ||
+      (rc = dalloc(&p.d_mask, (size_t)p.XN * p.YN, &B)) || (rc = dalloc(&p.d_tb, p.U + 1, &B)) ||
+      (rc = dalloc(&p.d_lut, p.M, &B)) || (rc = dalloc(&p.d_satx, nimg, &B)) ||
+      (rc = dalloc(&p.d_saty, nimg, &B)) || (rc = dalloc(&p.d_satq, nsino, &B)) ||
+      (rc = dalloc(&p.d_vg, p.PNmax, &B)) || (rc = dalloc(&p.d_fc, (size_t)p.PNmax * (p.U + 1), &B)) ||
+      (rc = dalloc(&p.d_cvd, (size_t)p.PNmax * p.U, &B)) ||
+      (rc = dalloc(&p.d_tmp, (size_t)p.XN * p.YN * p.Z, &B)) ||
+      (rc = dalloc(&p.d_angs, (size_t)p.PNmax, &B))) {
+    if (prev >= 0) cudaSetDevice(prev);
+    return rc;
+  }
+  std::vector<uint8_t> m((size_t)p.XN * p.YN, 1);
+  if (d.mask) std::memcpy(m.data(), d.mask, m.size());
+  p.has_mask = d.mask != nullptr;
+  cudaError_t e = cudaSuccess;
+  if (e == cudaSuccess) e = cudaMemcpy(p.d_bx, p.bx.data(), sizeof(double) * (p.U + 1), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(p.d_by, p.by.data(), sizeof(double) * (p.U + 1), cudaMemcpyHostToDevice);
+  std::vector<double> xd(p.xd.begin(), p.xd.end()), yd(p.yd.begin(), p.yd.end());
+  if (e == cudaSuccess) e = cudaMemcpy(p.d_xd, xd.data(), sizeof(double) * p.U, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(p.d_yd, yd.data(), sizeof(double) * p.U, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(p.d_mask, m.data(), m.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(p.d_tb, p.tb.data(), sizeof(float) * (p.U + 1), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(p.d_lut, p.lut.data(), sizeof(uint16_t) * p.M, cudaMemcpyHostToDevice);
+  if (prev >= 0) cudaSetDevice(prev);
+  if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "plan upload: %s", cudaGetErrorString(e));
+  *out = P.release();
+  return DDFAN_OK;
+}
+
+// ------------------------------------------------------------------ launches
+
+static int check_launch(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "%s launch: %s", what, cudaGetErrorString(e));
+  return DDFAN_OK;
+}
+
+static GeomConsts geom_consts(const Plan& p) {
+  GeomConsts g;
+  g.x0 = p.x0; g.y0 = p.y0; g.dx = p.dx; g.ocx = p.ocx; g.ocy = p.ocy;
+  g.bx = p.d_bx; g.by = p.d_by; g.xd = p.d_xd; g.yd = p.d_yd;
+  g.sh0x = p.sh0x; g.sh0y = p.sh0y;
+  g.U = p.U; g.XN = p.XN; g.YN = p.YN;
+  return g;
+}
+
+int launch_view_geom(const Plan& p, const float* d_angs, int stride, int PN, ViewGeom* vg,
+                     double2* fc, float* cvd, cudaStream_t st) {
+  if (PN < 1) return set_err(DDFAN_ERR_ARG, "PN must be >= 1");
+  k_view_geom<<<PN, 128, 0, st>>>(geom_consts(p), d_angs, stride, PN, vg, fc, cvd);
+  return check_launch("k_view_geom");
+}
+
+template <int M>
+static int sat_dispatch(const SatSrc& s, float4* out0, int nl0, float4* out1, int nl1, int N0, int N1,
+                        int Nw0, int Nw1, int ZB, int ntab, cudaStream_t st) {
+  const int Nw = std::max(Nw0, Nw1);
+  dim3 grid(std::max(nl0, nl1), (ZB + 7) / 8, ntab);
+  if (Nw <= 32 * 4) k_sat<M, 4><<<grid, 256, 0, st>>>(s, out0, nl0, nl1, out1, N0, N1, Nw0, Nw1, ZB);
+  else if (Nw <= 32 * 8) k_sat<M, 8><<<grid, 256, 0, st>>>(s, out0, nl0, nl1, out1, N0, N1, Nw0, Nw1, ZB);
+  else if (Nw <= 32 * 16) k_sat<M, 16><<<grid, 256, 0, st>>>(s, out0, nl0, nl1, out1, N0, N1, Nw0, Nw1, ZB);
+  else if (Nw <= 32 * 24) k_sat<M, 24><<<grid, 256, 0, st>>>(s, out0, nl0, nl1, out1, N0, N1, Nw0, Nw1, ZB);
+  else if (Nw <= 32 * 32) k_sat<M, 32><<<grid, 256, 0, st>>>(s, out0, nl0, nl1, out1, N0, N1, Nw0, Nw1, ZB);
+  else return set_err(DDFAN_ERR_UNSUPPORTED, "line of %d cells", Nw);
+  return check_launch("k_sat");
+}
+
+static int sat_launch(int mode, const SatSrc& s, float4* out0, int nl0, float4* out1, int nl1, int N0,
+                      int N1, int Nw0, int Nw1, int ZB, int ntab, cudaStream_t st) {
+  switch (mode) {
+    case SAT_FP32: return sat_dispatch<SAT_FP32>(s, out0, nl0, out1, nl1, N0, N1, Nw0, Nw1, ZB, ntab, st);
+    case SAT_HILO: return sat_dispatch<SAT_HILO>(s, out0, nl0, out1, nl1, N0, N1, Nw0, Nw1, ZB, ntab, st);
+    case SAT_FP64: return sat_dispatch<SAT_FP64>(s, out0, nl0, out1, nl1, N0, N1, Nw0, Nw1, ZB, ntab, st);
+  }
+  return set_err(DDFAN_ERR_ARG, "sat mode %d", mode);
+}
+
+// Both image tables (rows -> satx, columns -> saty) in one launch; the mask
+// multiply of AAPM_script/MultiSlicesProjGPU.cu:202-209 happens on load.
+int launch_sat_image(const Plan& p, const float* d_vol, cudaStream_t st) {
+  SatSrc s{};
+  s.kind = 0; s.a = d_vol; s.mask = p.has_mask ? p.d_mask : nullptr;
+  s.XN = p.XN; s.YN = p.YN; s.U = p.U; s.Z = p.Z;
+  return sat_launch(p.mode, s, p.d_satx, p.YN, p.d_saty, p.XN, p.XN, p.YN, p.XN, p.YN, p.ZB, 2, st);
+}
+
+int launch_sat_sino(const Plan& p, const float* d_prj, int PN, const float* wgt, float wscale,
+                    const float* y, const int* yview, const float* rowsum, cudaStream_t st) {
+  SatSrc s{};
+  s.kind = 2; s.a = d_prj; s.wgt = wgt; s.wscale = wscale; s.y = y; s.yview = yview;
+  s.rowsum = rowsum; s.XN = p.XN; s.YN = p.YN; s.U = p.U; s.Z = p.Z;
+  return sat_launch(p.mode, s, p.d_satq, PN, nullptr, 0, p.U, 0, p.U + 1, 0, p.ZB, 1, st);
+}
+
+constexpr int FWD_CG = 8;
+constexpr int BACK_VG = 8;
+
+template <int M, int ZL>
+static void fwd_go(const FwdArgs& a, cudaStream_t st) {
+  constexpr int NG = 32 / ZL;
+  dim3 grid((a.U + 4 * NG * FWD_CG - 1) / (4 * NG * FWD_CG), a.PN, (a.ZB + ZL - 1) / ZL);
+  k_fwd<M, ZL, FWD_CG><<<grid, 128, 0, st>>>(a);
+}
+
+template <int M>
+static void fwd_zl(int ZL, const FwdArgs& a, cudaStream_t st) {
+  switch (ZL) {
+    case 8: fwd_go<M, 8>(a, st); break;
+    case 4: fwd_go<M, 4>(a, st); break;
+    case 2: fwd_go<M, 2>(a, st); break;
+    default: fwd_go<M, 1>(a, st); break;
+  }
+}
+
+int launch_fwd(const Plan& p, const ViewGeom* vg, const double2* fc, const float* cvd,
+               const int* order, int PN, float* d_prj, int zlo, int zhi, cudaStream_t st) {
+  if (PN > 65535) return set_err(DDFAN_ERR_UNSUPPORTED, "more than 65535 views in one call");
+  FwdArgs a;
+  a.satx = p.d_satx; a.saty = p.d_saty; a.vg = vg; a.fc = fc; a.cvd = cvd; a.order = order;
+  a.out = d_prj; a.PN = PN; a.U = p.U; a.Z = p.Z; a.ZB = p.ZB; a.XN = p.XN; a.YN = p.YN;
+  a.dx = p.dx; a.zlo = zlo; a.zhi = zhi;
+  switch (p.mode) {
+    case SAT_FP32: fwd_zl<SAT_FP32>(p.ZL, a, st); break;
+    case SAT_HILO: fwd_zl<SAT_HILO>(p.ZL, a, st); break;
+    default: fwd_zl<SAT_FP64>(p.ZL, a, st); break;
+  }
+  return check_launch("k_fwd");
+}
+
+template <int M, int ZL>
+static void ref_go(const RefArgs& a, cudaStream_t st) {
+  constexpr int NG = 32 / ZL;
+  const int nseg = (a.XN + BACK_VG - 1) / BACK_VG;
+  dim3 grid((nseg * a.YN + 4 * NG - 1) / (4 * NG), 1, (a.ZB + ZL - 1) / ZL);
+  k_back_ref<M, ZL, BACK_VG><<<grid, 128, 0, st>>>(a);
+}
+
+template <int M, int ZL, bool XM>
+static void adj_go(const AdjArgs& a, cudaStream_t st) {
+  constexpr int NG = 32 / ZL;
+  const int nl = XM ? a.XN : a.YN, N = XM ? a.YN : a.XN;
+  const int nseg = (N + BACK_VG - 1) / BACK_VG;
+  dim3 grid((nseg * nl + 4 * NG - 1) / (4 * NG), 1, (a.ZB + ZL - 1) / ZL);
+  k_back_adj<M, ZL, BACK_VG, XM><<<grid, 128, 0, st>>>(a);
+}
+
+template <int M>
+static void ref_zl(int ZL, const RefArgs& a, cudaStream_t st) {
+  switch (ZL) {
+    case 8: ref_go<M, 8>(a, st); break;
+    case 4: ref_go<M, 4>(a, st); break;
+    case 2: ref_go<M, 2>(a, st); break;
+    default: ref_go<M, 1>(a, st); break;
+  }
+}
+
+template <int M, bool XM>
+static void adj_zl(int ZL, const AdjArgs& a, cudaStream_t st) {
+  switch (ZL) {
+    case 8: adj_go<M, 8, XM>(a, st); break;
+    case 4: adj_go<M, 4, XM>(a, st); break;
+    case 2: adj_go<M, 2, XM>(a, st); break;
+    default: adj_go<M, 1, XM>(a, st); break;
+  }
+}
+
+// Backprojection of the table in p.d_satq (built by launch_sat_sino with the
+// matching weights).  `epi` holds the final destination/update; ADJ runs two
+// passes (x-column lines, then y-row lines) through p.d_tmp.
+int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2* fc, int PN,
+                const BackEpi& epi, cudaStream_t st) {
+  if (back_mode == DDFAN_BACK_REF) {
+    RefArgs a;
+    a.satq = p.d_satq; a.vg = vg; a.PN = PN; a.U = p.U; a.Z = p.Z; a.ZB = p.ZB;
+    a.XN = p.XN; a.YN = p.YN; a.ocx = p.ocx; a.ocy = p.ocy; a.dx = p.dx;
+    a.inv_sid = p.inv_sid; a.inv_dbeta = p.inv_dbeta; a.cnt = (double)p.detCntIdx + 0.5;
+    a.epi = epi;
+    switch (p.mode) {
+      case SAT_FP32: ref_zl<SAT_FP32>(p.ZL, a, st); break;
+      case SAT_HILO: ref_zl<SAT_HILO>(p.ZL, a, st); break;
+      default: ref_zl<SAT_FP64>(p.ZL, a, st); break;
+    }
+    return check_launch("k_back_ref");
+  }
+  if (back_mode != DDFAN_BACK_ADJ) return set_err(DDFAN_ERR_ARG, "back_mode %d", back_mode);
+  if (!p.adj_ok) return set_err(DDFAN_ERR_UNSUPPORTED, "detector boundaries are not monotone as seen from the source");
+  AdjArgs a;
+  a.satq = p.d_satq; a.vg = vg; a.fc = fc; a.tb = p.d_tb; a.lut = p.d_lut;
+  a.t0 = p.t0; a.invdt = p.invdt; a.dirt = p.dirt; a.M = p.M;
+  a.PN = PN; a.U = p.U; a.Z = p.Z; a.ZB = p.ZB; a.XN = p.XN; a.YN = p.YN;
+  a.ocx = p.ocx; a.ocy = p.ocy; a.dx = p.dx;
+  // pass 1: x-major views, lines = x columns -> tmp (mask applied)
+  a.epi = epi;
+  a.epi.out = p.d_tmp; a.epi.addend = nullptr; a.epi.xin = nullptr; a.epi.colsum = nullptr;
+  a.epi.nonneg = 0;
+  switch (p.mode) {
+    case SAT_FP32: adj_zl<SAT_FP32, true>(p.ZL, a, st); break;
+    case SAT_HILO: adj_zl<SAT_HILO, true>(p.ZL, a, st); break;
+    default: adj_zl<SAT_FP64, true>(p.ZL, a, st); break;
+  }
+  int rc = check_launch("k_back_adj<x>");
+  if (rc) return rc;
+  // pass 2: y-major views, lines = y rows, plus pass 1, then the final epilogue
+  a.epi = epi;
+  a.epi.addend = p.d_tmp;
+  switch (p.mode) {
+    case SAT_FP32: adj_zl<SAT_FP32, false>(p.ZL, a, st); break;
+    case SAT_HILO: adj_zl<SAT_HILO, false>(p.ZL, a, st); break;
+    default: adj_zl<SAT_FP64, false>(p.ZL, a, st); break;
+  }
+  return check_launch("k_back_adj<y>");
+}
+
+// ------------------------------------------------------------------ device API
+
+int proj_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const float* d_vol, float* d_prj,
+                    int zlo, int zhi, cudaStream_t st) {
+  int rc;
+  if ((rc = launch_view_geom(p, d_angs, stride, PN, p.d_vg, p.d_fc, p.d_cvd, st))) return rc;
+  if ((rc = launch_sat_image(p, d_vol, st))) return rc;
+  return launch_fwd(p, p.d_vg, p.d_fc, p.d_cvd, nullptr, PN, d_prj, zlo, zhi, st);
+}
+
+int back_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const float* d_prj, float* d_vol,
+                    int back_mode, int zlo, int zhi, cudaStream_t st) {
+  int rc;
+  if ((rc = launch_view_geom(p, d_angs, stride, PN, p.d_vg, p.d_fc, p.d_cvd, st))) return rc;
+  const bool adj = back_mode == DDFAN_BACK_ADJ;
+  if ((rc = launch_sat_sino(p, d_prj, PN, adj ? p.d_cvd : nullptr, 1.f, nullptr, nullptr, nullptr, st)))
+    return rc;
+  BackEpi e{};
+  e.out = d_vol; e.mask = p.has_mask ? p.d_mask : nullptr; e.zlo = zlo; e.zhi = zhi;
+  return launch_back(p, back_mode, p.d_vg, p.d_fc, PN, e, st);
+}
+
+// Groups of slices sharing one angle list: per-slice angle arrays
+// (hangs[PN][SLN]) become one launch per distinct list.
+static void angle_groups(const float* hangs, int PN, int SLN, std::vector<std::vector<int>>& groups) {
+  groups.clear();
+  std::vector<int> rep;  // representative slice per group
+  for (int z = 0; z < SLN; ++z) {
+    int gi = -1;
+    for (size_t g = 0; g < rep.size() && gi < 0; ++g) {
+      const int r = rep[g];
+      bool same = true;
+      for (int q = 0; q < PN && same; ++q)
+        same = std::memcmp(&hangs[(size_t)q * SLN + z], &hangs[(size_t)q * SLN + r], sizeof(float)) == 0;
+      if (same) gi = (int)g;
+    }
+    if (gi < 0) {
+      rep.push_back(z);
+      groups.push_back({z});
+    } else {
+      groups[gi].push_back(z);
+    }
+  }
+}
+
+// Run `fn(angles-of-group, zlo, zhi)` once per group of slices with a common
+// angle list; slices outside [zlo, zhi) are computed but not written.
+template <class F>
+static int for_angle_groups(Plan& p, const float* h_angs, int PN, F&& fn, cudaStream_t st) {
+  std::vector<std::vector<int>> groups;
+  angle_groups(h_angs, PN, p.Z, groups);
+  std::vector<float> a(PN);
+  for (auto& g : groups) {
+    for (int q = 0; q < PN; ++q) a[q] = h_angs[(size_t)q * p.Z + g[0]];
+    cudaError_t e = cudaMemcpyAsync(p.d_angs, a.data(), sizeof(float) * PN, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "angles upload: %s", cudaGetErrorString(e));
+    // contiguous runs of the group
+    size_t i = 0;
+    while (i < g.size()) {
+      size_t j = i + 1;
+      while (j < g.size() && g[j] == g[j - 1] + 1) ++j;
+      int rc = fn(p.d_angs, g[i], g[j - 1] + 1);
+      if (rc) return rc;
+      i = j;
+    }
+    // the pageable source buffer `a` is reused: make the copy complete first
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "sync: %s", cudaGetErrorString(e));
+  }
+  return DDFAN_OK;
+}
+
+}  // namespace ddfan
+
+// ====================================================================== C ABI
+
+using namespace ddfan;
+
+extern "C" {
+
+DDFAN_API const char* ddfan_last_error(void) { return ddfan::last_error(); }
+DDFAN_API int ddfan_version(void) { return 1; }
+
+DDFAN_API int ddfan_fan_geometry(float sid, float sdd, int DNU, float detCellWidth, float detCntIdx,
+                                 float* x0, float* y0, float* xds, float* yds) {
+  if (DNU < 1 || !xds || !yds || !x0 || !y0) return set_err(DDFAN_ERR_ARG, "fan_geometry: bad arguments");
+  // AAPM_script/DD2MutiSlices.m:55-76, in MATLAB single arithmetic
+  const float stepTheta = atanf(detCellWidth / 2.0f / sdd) * 2.0f;
+  for (int ii = 1; ii <= DNU; ++ii) {
+    const float curBeta = ((float)ii - detCntIdx) * stepTheta;
+    xds[ii - 1] = sinf(curBeta) * sdd;
+    yds[ii - 1] = sid - cosf(curBeta) * sdd;
+  }
+  *x0 = 0.0f;
+  *y0 = sid;
+  return DDFAN_OK;
+}
+
+DDFAN_API int ddfan_plan_create(ddfan_plan** out, float x0, float y0, int DNU, const float* xds,
+                                const float* yds, float detCntIdx, float imgXCenter, float imgYCenter,
+                                int XN, int YN, float dx, const uint8_t* mask, int SLN, int PNmax,
+                                int sat_mode, int device) {
+  if (!out) return set_err(DDFAN_ERR_ARG, "out is null");
+  PlanDesc d{x0, y0, DNU, xds, yds, detCntIdx, imgXCenter, imgYCenter, XN, YN, dx, mask, SLN, PNmax,
+             sat_mode, device};
+  Plan* p = nullptr;
+  int rc = plan_create(&p, d);
+  *out = reinterpret_cast<ddfan_plan*>(p);
+  return rc;
+}
+
+DDFAN_API void ddfan_plan_destroy(ddfan_plan* plan) { plan_free(reinterpret_cast<Plan*>(plan)); }
+
+DDFAN_API size_t ddfan_plan_device_bytes(const ddfan_plan* plan) {
+  return plan ? reinterpret_cast<const Plan*>(plan)->bytes : 0;
+}
+
+DDFAN_API int ddfan_proj_dev(ddfan_plan* plan, const float* d_angs, int PN, int angs_per_slice,
+                             const float* d_vol, float* d_prj, void* stream) {
+  Plan* p = reinterpret_cast<Plan*>(plan);
+  if (!p || !d_angs || !d_vol || !d_prj) return set_err(DDFAN_ERR_ARG, "proj_dev: null argument");
+  if (PN < 1 || PN > p->PNmax) return set_err(DDFAN_ERR_ARG, "proj_dev: PN=%d outside [1, %d]", PN, p->PNmax);
+  cudaStream_t st = (cudaStream_t)stream;
+  DeviceGuard dg(p->device);
+  if (!angs_per_slice) return proj_dev_shared(*p, d_angs, 1, PN, d_vol, d_prj, 0, p->Z, st);
+  std::vector<float> h((size_t)PN * p->Z);
+  cudaError_t e = cudaMemcpyAsync(h.data(), d_angs, sizeof(float) * h.size(), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "angles download: %s", cudaGetErrorString(e));
+  return for_angle_groups(*p, h.data(), PN, [&](const float* da, int zlo, int zhi) {
+    return proj_dev_shared(*p, da, 1, PN, d_vol, d_prj, zlo, zhi, st);
+  }, st);
+}
+
+DDFAN_API int ddfan_back_dev(ddfan_plan* plan, const float* d_angs, int PN, int angs_per_slice,
+                             const float* d_prj, float* d_vol, int back_mode, void* stream) {
+  Plan* p = reinterpret_cast<Plan*>(plan);
+  if (!p || !d_angs || !d_vol || !d_prj) return set_err(DDFAN_ERR_ARG, "back_dev: null argument");
+  if (PN < 1 || PN > p->PNmax) return set_err(DDFAN_ERR_ARG, "back_dev: PN=%d outside [1, %d]", PN, p->PNmax);
+  if (back_mode != DDFAN_BACK_REF && back_mode != DDFAN_BACK_ADJ)
+    return set_err(DDFAN_ERR_ARG, "back_dev: back_mode %d", back_mode);
+  cudaStream_t st = (cudaStream_t)stream;
+  DeviceGuard dg(p->device);
+  if (!angs_per_slice) return back_dev_shared(*p, d_angs, 1, PN, d_prj, d_vol, back_mode, 0, p->Z, st);
+  std::vector<float> h((size_t)PN * p->Z);
+  cudaError_t e = cudaMemcpyAsync(h.data(), d_angs, sizeof(float) * h.size(), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "angles download: %s", cudaGetErrorString(e));
+  return for_angle_groups(*p, h.data(), PN, [&](const float* da, int zlo, int zhi) {
+    return back_dev_shared(*p, da, 1, PN, d_prj, d_vol, back_mode, zlo, zhi, st);
+  }, st);
+}
+
+}  // extern "C"

@@ -1,0 +1,88 @@
+// ddfan_plan.h -- host-side plan object and internal launch functions of libddfan.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "ddfan_device.cuh"
+
+namespace ddfan {
+
+struct BackEpi;
+
+int set_err(int code, const char* fmt, ...);
+const char* last_error();
+
+struct PlanDesc {
+  float x0, y0;
+  int DNU;
+  const float* xds;
+  const float* yds;
+  float detCntIdx, imgXCenter, imgYCenter;
+  int XN, YN;
+  float dx;
+  const uint8_t* mask;
+  int SLN, PNmax, sat_mode, device;
+};
+
+// Geometry and device scratch for one (image, detector, slice count) shape.
+struct Plan {
+  int device = 0;
+  int XN = 0, YN = 0, U = 0, Z = 0, ZB = 0, PNmax = 0, mode = 0, ZL = 1;
+  double x0 = 0, y0 = 0, dx = 1, ocx = 0, ocy = 0, detCntIdx = 0;
+  double inv_dbeta = 0, inv_sid = 0;  // REF backprojector
+  double sh0x = 0, sh0y = -1;         // unit vector source -> rotation centre, angle 0
+  float t0 = 0, invdt = 0, dirt = 1;  // exact-adjoint bracket table
+  int M = 0;
+  bool adj_ok = true, has_mask = false;
+  std::vector<double> bx, by;
+  std::vector<float> xd, yd, tb;
+  std::vector<uint16_t> lut;
+  // device
+  double *d_bx = nullptr, *d_by = nullptr, *d_xd = nullptr, *d_yd = nullptr;
+  uint8_t* d_mask = nullptr;
+  float* d_tb = nullptr;
+  uint16_t* d_lut = nullptr;
+  float4 *d_satx = nullptr, *d_saty = nullptr, *d_satq = nullptr;  // prefix-sum tables
+  ViewGeom* d_vg = nullptr;
+  double2* d_fc = nullptr;
+  float* d_cvd = nullptr;
+  float* d_tmp = nullptr;   // one image of scratch (exact adjoint, pass 1)
+  float* d_angs = nullptr;  // PNmax angles (host-angle entry points)
+  size_t bytes = 0;
+};
+
+int plan_create(Plan** out, const PlanDesc& d);
+void plan_free(Plan* p);
+
+int launch_view_geom(const Plan& p, const float* d_angs, int stride, int PN, ViewGeom* vg,
+                     double2* fc, float* cvd, cudaStream_t st);
+int launch_sat_image(const Plan& p, const float* d_vol, cudaStream_t st);
+int launch_sat_sino(const Plan& p, const float* d_prj, int PN, const float* wgt, float wscale,
+                    const float* y, const int* yview, const float* rowsum, cudaStream_t st);
+int launch_fwd(const Plan& p, const ViewGeom* vg, const double2* fc, const float* cvd,
+               const int* order, int PN, float* d_prj, int zlo, int zhi, cudaStream_t st);
+int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2* fc, int PN,
+                const BackEpi& epi, cudaStream_t st);
+int proj_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const float* d_vol,
+                    float* d_prj, int zlo, int zhi, cudaStream_t st);
+int back_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const float* d_prj,
+                    float* d_vol, int back_mode, int zlo, int zhi, cudaStream_t st);
+
+// Makes `dev` current for the scope and restores the caller's device.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+}  // namespace ddfan

@@ -1,0 +1,514 @@
+// ddfan_solver.cu -- mex-compatible host entry points and the device-resident
+// OS-SART / FISTA solver of libddfan.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "ddfan.h"
+#include "ddfan_kernels.cuh"
+#include "ddfan_plan.h"
+
+namespace ddfan {
+
+namespace {
+
+struct PlanPtr {
+  Plan* p = nullptr;
+  ~PlanPtr() { plan_free(p); }
+};
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  int alloc(size_t n) {
+    cudaError_t e = cudaMalloc((void**)&p, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      cudaGetLastError();
+      return set_err(DDFAN_ERR_NOMEM, "cudaMalloc(%zu): %s", n * sizeof(T), cudaGetErrorString(e));
+    }
+    return DDFAN_OK;
+  }
+};
+
+#define DDFAN_CK(call)                                                                         \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess)                                                                     \
+      return set_err(DDFAN_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                     __LINE__);                                                                \
+  } while (0)
+
+// Slabs of slices per device, as startIdx describes them
+// (AAPM_script/DD2MutiSlices.m:95-101, MultiSlicesProjGPU.cu:500-514).
+int slabs_of(const int32_t* startIdx, int n, int SLN, std::vector<std::pair<int, int>>& out) {
+  out.clear();
+  if (!startIdx || n <= 0) {
+    out.emplace_back(0, SLN);
+    return DDFAN_OK;
+  }
+  for (int k = 0; k < n; ++k) {
+    const int a = startIdx[k], b = k + 1 < n ? startIdx[k + 1] : SLN;
+    if (a < 0 || b > SLN || a > b) return set_err(DDFAN_ERR_ARG, "startIdx[%d]=%d: slabs must be increasing within [0, %d]", k, a, SLN);
+    if (k == 0 && a != 0) return set_err(DDFAN_ERR_ARG, "startIdx[0] must be 0");
+    if (b > a) out.emplace_back(a, b);
+  }
+  return DDFAN_OK;
+}
+
+// gather slices [a, b) of a [rows][SLN] array into [rows][b - a]
+void gather_slab(const float* src, size_t rows, int SLN, int a, int b, std::vector<float>& dst) {
+  const int n = b - a;
+  dst.resize(rows * n);
+  for (size_t r = 0; r < rows; ++r) std::memcpy(&dst[r * n], src + r * SLN + a, sizeof(float) * n);
+}
+
+void scatter_slab(const std::vector<float>& src, size_t rows, int SLN, int a, int b, float* dst) {
+  const int n = b - a;
+  for (size_t r = 0; r < rows; ++r) std::memcpy(dst + r * SLN + a, &src[r * n], sizeof(float) * n);
+}
+
+int device_count() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+}  // namespace
+
+// One slab of a mex-style call on one device: upload, project or backproject
+// (one launch group per distinct angle list), download.
+static int mex_slab(bool forward, const PlanDesc& d, const float* angs, int PN, const float* in,
+                    float* out, int back_mode) {
+  PlanPtr P;
+  int rc = plan_create(&P.p, d);
+  if (rc) return rc;
+  Plan& p = *P.p;
+  DeviceGuard g(p.device);
+  const size_t V = (size_t)p.XN * p.YN * p.Z, S = (size_t)PN * p.U * p.Z;
+  DevBuf<float> din, dout;
+  if ((rc = din.alloc(forward ? V : S)) || (rc = dout.alloc(forward ? S : V))) return rc;
+  DDFAN_CK(cudaMemcpy(din.p, in, sizeof(float) * (forward ? V : S), cudaMemcpyHostToDevice));
+  // per-slice angle lists: one launch group per distinct list
+  std::vector<int> rep;
+  std::vector<std::vector<int>> grp;
+  for (int z = 0; z < p.Z; ++z) {
+    int gi = -1;
+    for (size_t k = 0; k < rep.size() && gi < 0; ++k) {
+      bool same = true;
+      for (int q = 0; q < PN && same; ++q)
+        same = std::memcmp(&angs[(size_t)q * p.Z + z], &angs[(size_t)q * p.Z + rep[k]], sizeof(float)) == 0;
+      if (same) gi = (int)k;
+    }
+    if (gi < 0) { rep.push_back(z); grp.push_back({z}); }
+    else grp[gi].push_back(z);
+  }
+  std::vector<float> a(PN);
+  for (auto& gr : grp) {
+    for (int q = 0; q < PN; ++q) a[q] = angs[(size_t)q * p.Z + gr[0]];
+    DDFAN_CK(cudaMemcpy(p.d_angs, a.data(), sizeof(float) * PN, cudaMemcpyHostToDevice));
+    size_t i = 0;
+    while (i < gr.size()) {
+      size_t j = i + 1;
+      while (j < gr.size() && gr[j] == gr[j - 1] + 1) ++j;
+      rc = forward ? proj_dev_shared(p, p.d_angs, 1, PN, din.p, dout.p, gr[i], gr[j - 1] + 1, 0)
+                   : back_dev_shared(p, p.d_angs, 1, PN, din.p, dout.p, back_mode, gr[i], gr[j - 1] + 1, 0);
+      if (rc) return rc;
+      i = j;
+    }
+    DDFAN_CK(cudaDeviceSynchronize());
+  }
+  DDFAN_CK(cudaMemcpy(out, dout.p, sizeof(float) * (forward ? S : V), cudaMemcpyDeviceToHost));
+  return DDFAN_OK;
+}
+
+static int mex_call(bool forward, float x0, float y0, int DNU, const float* xds, const float* yds,
+                    float detCntIdx, float imgXCenter, float imgYCenter, const float* hangs, int PN,
+                    int XN, int YN, int SLN, const float* in, float dx, const uint8_t* mask,
+                    const int32_t* startIdx, int nStartIdx, int sat_mode, int back_mode, float* out) {
+  if (!xds || !yds || !hangs || !in || !out) return set_err(DDFAN_ERR_ARG, "null argument");
+  if (PN < 1 || SLN < 1 || XN < 1 || YN < 1 || DNU < 2) return set_err(DDFAN_ERR_ARG, "bad sizes");
+  std::vector<std::pair<int, int>> slabs;
+  int rc = slabs_of(startIdx, nStartIdx, SLN, slabs);
+  if (rc) return rc;
+  const int ndev = device_count();
+  if (ndev < 1) return set_err(DDFAN_ERR_CUDA, "no CUDA device");
+  const size_t npix = (size_t)XN * YN, nray = (size_t)PN * DNU;
+  for (size_t k = 0; k < slabs.size(); ++k) {
+    const int a = slabs[k].first, b = slabs[k].second, n = b - a;
+    PlanDesc d{x0, y0, DNU, xds, yds, detCntIdx, imgXCenter, imgYCenter, XN, YN, dx, mask, n, PN,
+               sat_mode, (int)(k % ndev)};
+    if (n == SLN) {
+      rc = mex_slab(forward, d, hangs, PN, in, out, back_mode);
+    } else {
+      std::vector<float> sin, sang, sout(forward ? nray * n : npix * n);
+      gather_slab(in, forward ? npix : nray, SLN, a, b, sin);
+      gather_slab(hangs, PN, SLN, a, b, sang);
+      rc = mex_slab(forward, d, sang.data(), PN, sin.data(), sout.data(), back_mode);
+      if (!rc) scatter_slab(sout, forward ? nray : npix, SLN, a, b, out);
+    }
+    if (rc) return rc;
+  }
+  return DDFAN_OK;
+}
+
+// ====================================================================== solver
+
+struct Solver {
+  Plan* P = nullptr;  // SLN slices, PNmax = largest subset
+  int device = 0;
+  int PNall = 0, nsub = 1, useFISTA = 1, nonneg = 0, back_mode = DDFAN_BACK_REF;
+  int XN = 0, YN = 0, U = 0, Z = 0;
+  std::vector<int> off, cnt;  // subset k: rows [off[k], off[k] + cnt[k]) of the subset-ordered tables
+  ViewGeom* d_vg = nullptr;
+  double2* d_fc = nullptr;
+  float* d_cvd = nullptr;
+  int* d_yview = nullptr;  // subset-ordered row -> original view index
+  int* d_order = nullptr;  // per subset: forward CTA order (x-major views first)
+  float* d_rows = nullptr; // [PNall][U]   row sums, subset order
+  float* d_cols = nullptr; // [nsub][YN][XN] column sums
+  float* d_y = nullptr;    // [PNall][U][Z] measured sinogram, original order
+  float* d_x = nullptr;
+  float* d_xprev = nullptr;
+  float* d_ax = nullptr;   // [PNmax][U][Z]
+  double* d_t = nullptr;
+  cudaStream_t own = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  size_t bytes = 0;
+  int launches = 0;
+};
+
+static void solver_free(Solver* s) {
+  if (!s) return;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(s->device);
+  if (s->gexec) cudaGraphExecDestroy(s->gexec);
+  if (s->graph) cudaGraphDestroy(s->graph);
+  if (s->own) cudaStreamDestroy(s->own);
+  void* ptrs[] = {s->d_vg, s->d_fc, s->d_cvd, s->d_yview, s->d_order, s->d_rows, s->d_cols,
+                  s->d_y, s->d_x, s->d_xprev, s->d_ax, s->d_t};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  plan_free(s->P);
+  if (prev >= 0) cudaSetDevice(prev);
+  delete s;
+}
+
+template <class T>
+static int salloc(Solver& s, T** p, size_t n) {
+  cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return set_err(DDFAN_ERR_NOMEM, "solver cudaMalloc(%zu): %s", n * sizeof(T), cudaGetErrorString(e));
+  }
+  s.bytes += std::max<size_t>(n, 1) * sizeof(T);
+  return DDFAN_OK;
+}
+
+// One OS-SART iteration (AAPM_script/OSSART_AAPM.m:79-115) on stream st.
+static int solver_iteration(Solver& s, cudaStream_t st) {
+  Plan& p = *s.P;
+  int rc, n = 0;
+  const bool adj = s.back_mode == DDFAN_BACK_ADJ;
+  for (int k = 0; k < s.nsub; ++k) {
+    const int o = s.off[k], c = s.cnt[k];
+    const ViewGeom* vg = s.d_vg + o;
+    const double2* fc = s.d_fc + (size_t)o * (s.U + 1);
+    const float* cvd = s.d_cvd + (size_t)o * s.U;
+    // project the current image (:85)
+    if ((rc = launch_sat_image(p, s.d_x, st))) return rc;
+    if ((rc = launch_fwd(p, vg, fc, cvd, s.d_order + o, c, s.d_ax, 0, s.Z, st))) return rc;
+    // residual (y - A x) / rowSum folded into the sinogram prefix sums (:86-88)
+    if ((rc = launch_sat_sino(p, s.d_ax, c, adj ? cvd : nullptr, 1.f, s.d_y, s.d_yview + o,
+                              s.d_rows + (size_t)o * s.U, st)))
+      return rc;
+    // backproject, divide by colSum, add, optional clamp (:91-97)
+    BackEpi e{};
+    e.out = s.d_x; e.xin = s.d_x; e.colsum = s.d_cols + (size_t)k * s.XN * s.YN;
+    e.nonneg = s.nonneg; e.mask = p.has_mask ? p.d_mask : nullptr; e.zlo = 0; e.zhi = s.Z;
+    if ((rc = launch_back(p, s.back_mode, vg, fc, c, e, st))) return rc;
+    n += adj ? 5 : 4;
+  }
+  if (s.useFISTA) {
+    const size_t V = (size_t)s.XN * s.YN * s.Z;
+    const int blocks = (int)std::min<size_t>((V + 255) / 256, 148 * 16);
+    k_fista<<<blocks, 256, 0, st>>>(s.d_x, s.d_xprev, V, s.d_t);
+    k_fista_t<<<1, 1, 0, st>>>(s.d_t);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "fista launch: %s", cudaGetErrorString(e));
+    n += 2;
+  }
+  s.launches = n;
+  return DDFAN_OK;
+}
+
+static int solver_create(Solver** out, float x0, float y0, int DNU, const float* xds, const float* yds,
+                         float detCntIdx, float imgXCenter, float imgYCenter, const float* hangs,
+                         int PNall, int XN, int YN, int SLN, float dx, const uint8_t* mask,
+                         int numOfOS, int useFISTA, int nonneg, int sat_mode, int back_mode,
+                         int device) {
+  *out = nullptr;
+  if (!hangs || !xds || !yds) return set_err(DDFAN_ERR_ARG, "null argument");
+  if (numOfOS < 1 || numOfOS > PNall) return set_err(DDFAN_ERR_ARG, "numOfOS=%d outside [1, %d]", numOfOS, PNall);
+  if (back_mode != DDFAN_BACK_REF && back_mode != DDFAN_BACK_ADJ)
+    return set_err(DDFAN_ERR_ARG, "back_mode %d", back_mode);
+  // the device solver shares one angle list across slices
+  for (int q = 0; q < PNall; ++q)
+    for (int z = 1; z < SLN; ++z)
+      if (std::memcmp(&hangs[(size_t)q * SLN + z], &hangs[(size_t)q * SLN], sizeof(float)) != 0)
+        return set_err(DDFAN_ERR_UNSUPPORTED, "solver: view %d has per-slice angles", q);
+  std::unique_ptr<Solver, void (*)(Solver*)> S(new Solver(), solver_free);
+  Solver& s = *S;
+  s.device = device; s.PNall = PNall; s.nsub = numOfOS; s.useFISTA = useFISTA ? 1 : 0;
+  s.nonneg = nonneg ? 1 : 0; s.back_mode = back_mode; s.XN = XN; s.YN = YN; s.U = DNU; s.Z = SLN;
+  // subsets k, k + numOfOS, ... (AAPM_script/OSSART_AAPM.m:60)
+  std::vector<int> yview;
+  std::vector<float> angs;
+  int PNmax = 0;
+  for (int k = 0; k < numOfOS; ++k) {
+    s.off.push_back((int)yview.size());
+    for (int v = k; v < PNall; v += numOfOS) {
+      yview.push_back(v);
+      angs.push_back(hangs[(size_t)v * SLN]);
+    }
+    s.cnt.push_back((int)yview.size() - s.off.back());
+    PNmax = std::max(PNmax, s.cnt.back());
+  }
+  PlanDesc d{x0, y0, DNU, xds, yds, detCntIdx, imgXCenter, imgYCenter, XN, YN, dx, mask, SLN, PNmax,
+             sat_mode, device};
+  int rc = plan_create(&s.P, d);
+  if (rc) return rc;
+  s.bytes = s.P->bytes;
+  DeviceGuard g(device);
+  const size_t V = (size_t)XN * YN * SLN;
+  if ((rc = salloc(s, &s.d_vg, PNall)) || (rc = salloc(s, &s.d_fc, (size_t)PNall * (DNU + 1))) ||
+      (rc = salloc(s, &s.d_cvd, (size_t)PNall * DNU)) || (rc = salloc(s, &s.d_yview, PNall)) ||
+      (rc = salloc(s, &s.d_order, PNall)) || (rc = salloc(s, &s.d_rows, (size_t)PNall * DNU)) ||
+      (rc = salloc(s, &s.d_cols, (size_t)numOfOS * XN * YN)) ||
+      (rc = salloc(s, &s.d_y, (size_t)PNall * DNU * SLN)) || (rc = salloc(s, &s.d_x, V)) ||
+      (rc = salloc(s, &s.d_xprev, V)) || (rc = salloc(s, &s.d_ax, (size_t)PNmax * DNU * SLN)) ||
+      (rc = salloc(s, &s.d_t, 1)))
+    return rc;
+  DDFAN_CK(cudaStreamCreateWithFlags(&s.own, cudaStreamNonBlocking));
+  cudaStream_t st = s.own;
+  // per-view tables for every view, in subset order
+  DevBuf<float> dang;
+  if ((rc = dang.alloc(PNall))) return rc;
+  DDFAN_CK(cudaMemcpyAsync(dang.p, angs.data(), sizeof(float) * PNall, cudaMemcpyHostToDevice, st));
+  DDFAN_CK(cudaMemcpyAsync(s.d_yview, yview.data(), sizeof(int) * PNall, cudaMemcpyHostToDevice, st));
+  if ((rc = launch_view_geom(*s.P, dang.p, 1, PNall, s.d_vg, s.d_fc, s.d_cvd, st))) return rc;
+  // forward CTA order per subset: views of one orientation together (one
+  // image table at a time stays hot in L2)
+  std::vector<ViewGeom> hvg(PNall);
+  DDFAN_CK(cudaMemcpyAsync(hvg.data(), s.d_vg, sizeof(ViewGeom) * PNall, cudaMemcpyDeviceToHost, st));
+  DDFAN_CK(cudaStreamSynchronize(st));
+  std::vector<int> order(PNall);
+  for (int k = 0; k < numOfOS; ++k) {
+    int w = s.off[k];
+    for (int pass = 1; pass >= 0; --pass)
+      for (int i = 0; i < s.cnt[k]; ++i)
+        if (hvg[s.off[k] + i].xmajor == pass) order[w++] = i;
+  }
+  DDFAN_CK(cudaMemcpyAsync(s.d_order, order.data(), sizeof(int) * PNall, cudaMemcpyHostToDevice, st));
+  // row / column sums from slice 0 on a one-slice plan (AAPM_script/OSSART_AAPM.m:59-66)
+  {
+    PlanDesc d1 = d;
+    d1.SLN = 1;
+    PlanPtr P1;
+    if ((rc = plan_create(&P1.p, d1))) return rc;
+    DevBuf<float> ones, tmp;
+    const size_t n1 = std::max((size_t)XN * YN, (size_t)PNmax * DNU);
+    if ((rc = ones.alloc(n1)) || (rc = tmp.alloc((size_t)PNmax * DNU))) return rc;
+    std::vector<float> h1(n1, 1.0f);
+    DDFAN_CK(cudaMemcpyAsync(ones.p, h1.data(), sizeof(float) * n1, cudaMemcpyHostToDevice, st));
+    if ((rc = launch_sat_image(*P1.p, ones.p, st))) return rc;
+    for (int k = 0; k < numOfOS; ++k) {
+      const int o = s.off[k], c = s.cnt[k];
+      if ((rc = launch_fwd(*P1.p, s.d_vg + o, s.d_fc + (size_t)o * (DNU + 1), s.d_cvd + (size_t)o * DNU,
+                           nullptr, c, s.d_rows + (size_t)o * DNU, 0, 1, st)))
+        return rc;
+    }
+    for (int k = 0; k < numOfOS; ++k) {
+      const int o = s.off[k], c = s.cnt[k];
+      const bool adj = back_mode == DDFAN_BACK_ADJ;
+      if ((rc = launch_sat_sino(*P1.p, ones.p, c, adj ? s.d_cvd + (size_t)o * DNU : nullptr, 1.f,
+                                nullptr, nullptr, nullptr, st)))
+        return rc;
+      BackEpi e{};
+      e.out = s.d_cols + (size_t)k * XN * YN;
+      e.mask = P1.p->has_mask ? P1.p->d_mask : nullptr;
+      e.zlo = 0; e.zhi = 1;
+      if ((rc = launch_back(*P1.p, back_mode, s.d_vg + o, s.d_fc + (size_t)o * (DNU + 1), c, e, st)))
+        return rc;
+    }
+    DDFAN_CK(cudaStreamSynchronize(st));
+  }
+  const double one = 1.0;
+  DDFAN_CK(cudaMemcpyAsync(s.d_t, &one, sizeof(double), cudaMemcpyHostToDevice, st));
+  DDFAN_CK(cudaMemsetAsync(s.d_x, 0, sizeof(float) * V, st));
+  DDFAN_CK(cudaMemsetAsync(s.d_xprev, 0, sizeof(float) * V, st));
+  DDFAN_CK(cudaStreamSynchronize(st));
+  *out = S.release();
+  return DDFAN_OK;
+}
+
+}  // namespace ddfan
+
+using namespace ddfan;
+
+extern "C" {
+
+DDFAN_API int ddfan_MultiSlicesProjGPU(float x0, float y0, int DNU, const float* xds, const float* yds,
+                                       float imgXCenter, float imgYCenter, const float* hangs, int PN,
+                                       int XN, int YN, int SLN, const float* vol, float dx,
+                                       const uint8_t* mask, const int32_t* startIdx, int nStartIdx,
+                                       int sat_mode, float* prj) {
+  return mex_call(true, x0, y0, DNU, xds, yds, 0.f, imgXCenter, imgYCenter, hangs, PN, XN, YN, SLN,
+                  vol, dx, mask, startIdx, nStartIdx, sat_mode, DDFAN_BACK_REF, prj);
+}
+
+DDFAN_API int ddfan_MultiSlicesBackGPU(float x0, float y0, int DNU, const float* xds, const float* yds,
+                                       float detCntIdx, float imgXCenter, float imgYCenter,
+                                       const float* hangs, int PN, int XN, int YN, int SLN,
+                                       const float* prj, float dx, const uint8_t* mask,
+                                       const int32_t* startIdx, int nStartIdx, int sat_mode,
+                                       int back_mode, float* vol) {
+  if (back_mode != DDFAN_BACK_REF && back_mode != DDFAN_BACK_ADJ)
+    return set_err(DDFAN_ERR_ARG, "back_mode %d", back_mode);
+  return mex_call(false, x0, y0, DNU, xds, yds, detCntIdx, imgXCenter, imgYCenter, hangs, PN, XN, YN,
+                  SLN, prj, dx, mask, startIdx, nStartIdx, sat_mode, back_mode, vol);
+}
+
+DDFAN_API int ddfan_ossart_create(ddfan_ossart** out, float x0, float y0, int DNU, const float* xds,
+                                  const float* yds, float detCntIdx, float imgXCenter, float imgYCenter,
+                                  const float* hangs, int PNall, int XN, int YN, int SLN, float dx,
+                                  const uint8_t* mask, int numOfOS, int useFISTA, int nonneg,
+                                  int sat_mode, int back_mode, int device) {
+  if (!out) return set_err(DDFAN_ERR_ARG, "out is null");
+  Solver* s = nullptr;
+  int rc = solver_create(&s, x0, y0, DNU, xds, yds, detCntIdx, imgXCenter, imgYCenter, hangs, PNall,
+                         XN, YN, SLN, dx, mask, numOfOS, useFISTA, nonneg, sat_mode, back_mode, device);
+  *out = reinterpret_cast<ddfan_ossart*>(s);
+  return rc;
+}
+
+DDFAN_API void ddfan_ossart_destroy(ddfan_ossart* s) { solver_free(reinterpret_cast<Solver*>(s)); }
+
+DDFAN_API size_t ddfan_ossart_device_bytes(const ddfan_ossart* s) {
+  return s ? reinterpret_cast<const Solver*>(s)->bytes : 0;
+}
+
+DDFAN_API int ddfan_ossart_set_sinogram(ddfan_ossart* h, const float* proj, int is_device, void* stream) {
+  Solver* s = reinterpret_cast<Solver*>(h);
+  if (!s || !proj) return set_err(DDFAN_ERR_ARG, "null argument");
+  DeviceGuard g(s->device);
+  const size_t n = (size_t)s->PNall * s->U * s->Z;
+  DDFAN_CK(cudaMemcpyAsync(s->d_y, proj, sizeof(float) * n,
+                           is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                           (cudaStream_t)stream));
+  return DDFAN_OK;
+}
+
+DDFAN_API int ddfan_ossart_set_image(ddfan_ossart* h, const float* img, int is_device, void* stream) {
+  Solver* s = reinterpret_cast<Solver*>(h);
+  if (!s || !img) return set_err(DDFAN_ERR_ARG, "null argument");
+  DeviceGuard g(s->device);
+  const size_t n = (size_t)s->XN * s->YN * s->Z;
+  cudaStream_t st = (cudaStream_t)stream;
+  DDFAN_CK(cudaMemcpyAsync(s->d_x, img, sizeof(float) * n,
+                           is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+  DDFAN_CK(cudaMemcpyAsync(s->d_xprev, s->d_x, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+  static const double one = 1.0;
+  DDFAN_CK(cudaMemcpyAsync(s->d_t, &one, sizeof(double), cudaMemcpyHostToDevice, st));
+  // the pageable host sources above must be consumed before returning
+  DDFAN_CK(cudaStreamSynchronize(st));
+  return DDFAN_OK;
+}
+
+DDFAN_API int ddfan_ossart_iterate(ddfan_ossart* h, int numOfIter, int use_graph, void* stream) {
+  Solver* s = reinterpret_cast<Solver*>(h);
+  if (!s || numOfIter < 0) return set_err(DDFAN_ERR_ARG, "bad argument");
+  DeviceGuard g(s->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!use_graph) {
+    for (int it = 0; it < numOfIter; ++it) {
+      int rc = solver_iteration(*s, st);
+      if (rc) return rc;
+    }
+    return DDFAN_OK;
+  }
+  if (!s->gexec) {
+    DDFAN_CK(cudaStreamBeginCapture(s->own, cudaStreamCaptureModeThreadLocal));
+    int rc = solver_iteration(*s, s->own);
+    cudaGraph_t gr = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->own, &gr);
+    if (rc) {
+      if (gr) cudaGraphDestroy(gr);
+      return rc;
+    }
+    if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    s->graph = gr;
+    DDFAN_CK(cudaGraphInstantiate(&s->gexec, s->graph, 0));
+  }
+  for (int it = 0; it < numOfIter; ++it) DDFAN_CK(cudaGraphLaunch(s->gexec, st));
+  return DDFAN_OK;
+}
+
+DDFAN_API int ddfan_ossart_get_image(ddfan_ossart* h, float* img, int is_device, void* stream) {
+  Solver* s = reinterpret_cast<Solver*>(h);
+  if (!s || !img) return set_err(DDFAN_ERR_ARG, "null argument");
+  DeviceGuard g(s->device);
+  const size_t n = (size_t)s->XN * s->YN * s->Z;
+  cudaStream_t st = (cudaStream_t)stream;
+  DDFAN_CK(cudaMemcpyAsync(img, s->d_x, sizeof(float) * n,
+                           is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+  if (!is_device) DDFAN_CK(cudaStreamSynchronize(st));
+  return DDFAN_OK;
+}
+
+DDFAN_API float* ddfan_ossart_image_ptr(ddfan_ossart* h) {
+  Solver* s = reinterpret_cast<Solver*>(h);
+  return s ? s->d_x : nullptr;
+}
+
+DDFAN_API int ddfan_ossart_launches_per_iter(const ddfan_ossart* h) {
+  const Solver* s = reinterpret_cast<const Solver*>(h);
+  if (!s) return 0;
+  return s->nsub * (s->back_mode == DDFAN_BACK_ADJ ? 5 : 4) + (s->useFISTA ? 2 : 0);
+}
+
+DDFAN_API int ddfan_OSSART_AAPM(float x0, float y0, int DNU, const float* xds, const float* yds,
+                                float detCntIdx, float imgXCenter, float imgYCenter, const float* proj,
+                                const float* hangs, int PNall, int XN, int YN, int SLN, float dx,
+                                const float* initImg, const uint8_t* mask, int numOfIter, int numOfOS,
+                                int useFISTA, int nonneg, int sat_mode, int back_mode, float* reconImg) {
+  if (!proj || !initImg || !reconImg) return set_err(DDFAN_ERR_ARG, "null argument");
+  int dev = 0;
+  cudaGetDevice(&dev);
+  Solver* s = nullptr;
+  int rc = solver_create(&s, x0, y0, DNU, xds, yds, detCntIdx, imgXCenter, imgYCenter, hangs, PNall, XN,
+                         YN, SLN, dx, mask, numOfOS, useFISTA, nonneg, sat_mode, back_mode, dev);
+  if (rc) return rc;
+  ddfan_ossart* h = reinterpret_cast<ddfan_ossart*>(s);
+  if (!rc) rc = ddfan_ossart_set_sinogram(h, proj, 0, s->own);
+  if (!rc) rc = ddfan_ossart_set_image(h, initImg, 0, s->own);
+  if (!rc) rc = ddfan_ossart_iterate(h, numOfIter, 1, s->own);
+  if (!rc) rc = ddfan_ossart_get_image(h, reconImg, 0, s->own);
+  solver_free(s);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,160 @@
+/*
+ * ddfan.h -- C ABI of the B200 fan-beam multi-slice distance-driven (DD)
+ * projector / backprojector and OS-SART solver (libddfan.so).
+ *
+ * Every entry point returns a status code (DDFAN_OK on success) and never
+ * exits the process; ddfan_last_error() gives a message for the calling
+ * thread's last failure.  No entry point resets a device.
+ *
+ * Array layouts are the C (row-major) views of the reference's MATLAB arrays,
+ * so buffers pass through unchanged:
+ *   image    vol [YN][XN][SLN]   float   (MATLAB single(SLN, XN, YN))
+ *   sinogram prj [PN][DNU][SLN]  float   (MATLAB single(SLN, DNU, PN))
+ *   angles   hangs[PN][SLN]      float   (MATLAB single(SLN, PN)), radians
+ *   mask     mask [YN][XN]       uint8   (first XN*YN bytes of MATLAB [mask, mask'])
+ * Reference paths below are relative to the reference project root.
+ */
+#ifndef DDFAN_H
+#define DDFAN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define DDFAN_API __attribute__((visibility("default")))
+#else
+#define DDFAN_API
+#endif
+
+/* status codes */
+#define DDFAN_OK 0
+#define DDFAN_ERR_ARG 1         /* invalid argument (sizes, null pointers, modes) */
+#define DDFAN_ERR_CUDA 2        /* a CUDA runtime call failed */
+#define DDFAN_ERR_NOMEM 3       /* device or host allocation failed / over budget */
+#define DDFAN_ERR_UNSUPPORTED 4 /* geometry or size outside what the kernels handle */
+#define DDFAN_ERR_BUSY 5        /* resource in use (serving slots) */
+
+/* precision of the prefix-sum (SAT) tables and of their differences */
+#define DDFAN_SAT_FP32 0 /* plain FP32 sums (the reference's precision class) */
+#define DDFAN_SAT_HILO 1 /* compensated hi/lo FP32 pairs */
+#define DDFAN_SAT_FP64 2 /* FP64 sums */
+
+/* backprojector */
+#define DDFAN_BACK_REF 0 /* the reference backprojector's formula (MultiSlicesBackGPU.cu:115-184) */
+#define DDFAN_BACK_ADJ 1 /* exact transpose of the forward projector */
+
+DDFAN_API const char* ddfan_last_error(void);
+DDFAN_API int ddfan_version(void);
+
+/* Source position and channel centres on the arc detector, as the MATLAB
+ * wrapper builds them (replaces AAPM_script/DD2MutiSlices.m:49-76):
+ * stepTheta = 2 atan(detCellWidth / 2 / sdd), beta_i = (i - detCntIdx) stepTheta
+ * for 1-based i, xds_i = sdd sin(beta_i), yds_i = sid - sdd cos(beta_i),
+ * source (x0, y0) = (0, sid).  Single-precision arithmetic like MATLAB's. */
+DDFAN_API int ddfan_fan_geometry(float sid, float sdd, int DNU, float detCellWidth, float detCntIdx,
+                                 float* x0, float* y0, float* xds, float* yds);
+
+/* ---- mex-compatible host entry points (host pointers, synchronous) ----
+ * Replaces the MEX function MultiSlicesProjGPU
+ * (AAPM_script/MultiSlicesProjGPU.cu:550-575 -> DD2ProjMultiGPUs_CPP17 :486-547):
+ * the same 16 inputs in the same order, then the SAT precision and the output
+ * buffer prj[PN][DNU][SLN] (the mex allocates it; here the caller does).
+ * startIdx[nStartIdx] gives the first slice of each device's slab
+ * (DD2MutiSlices.m:95-101); slabs run on devices 0..nStartIdx-1 in turn,
+ * nStartIdx <= 0 or startIdx == NULL means one slab on the current device. */
+DDFAN_API int ddfan_MultiSlicesProjGPU(float x0, float y0, int DNU, const float* xds,
+                                       const float* yds, float imgXCenter, float imgYCenter,
+                                       const float* hangs, int PN, int XN, int YN, int SLN,
+                                       const float* vol, float dx, const uint8_t* mask,
+                                       const int32_t* startIdx, int nStartIdx, int sat_mode,
+                                       float* prj);
+
+/* Replaces the MEX function MultiSlicesBackGPU
+ * (AAPM_script/MultiSlicesBackGPU.cu:409-436 -> DD2BackMultiGPUs :349-406):
+ * the same 17 inputs in the same order, then SAT precision, backprojector
+ * (DDFAN_BACK_REF reproduces the reference; DDFAN_BACK_ADJ is the exact
+ * transpose of ddfan_MultiSlicesProjGPU) and the output vol[YN][XN][SLN].
+ * Voxels whose mask byte is 0 are written as 0. */
+DDFAN_API int ddfan_MultiSlicesBackGPU(float x0, float y0, int DNU, const float* xds,
+                                       const float* yds, float detCntIdx, float imgXCenter,
+                                       float imgYCenter, const float* hangs, int PN, int XN,
+                                       int YN, int SLN, const float* prj, float dx,
+                                       const uint8_t* mask, const int32_t* startIdx,
+                                       int nStartIdx, int sat_mode, int back_mode, float* vol);
+
+/* ---- device API: a plan owns the geometry and the scratch tables ----
+ * Replaces the per-call set-up of DD2::DD2_gpu_proj_branchless_sat2d
+ * (AAPM_script/MultiSlicesProjGPU.cu:211-385) and DD2_gpu_back
+ * (AAPM_script/MultiSlicesBackGPU.cu:187-268): boundaries, image-centre
+ * index, mask upload and table allocation happen once, not per call. */
+typedef struct ddfan_plan_s ddfan_plan;
+
+DDFAN_API int ddfan_plan_create(ddfan_plan** out, float x0, float y0, int DNU, const float* xds,
+                                const float* yds, float detCntIdx, float imgXCenter,
+                                float imgYCenter, int XN, int YN, float dx,
+                                const uint8_t* mask /* host [YN][XN], NULL = all ones */,
+                                int SLN, int PNmax, int sat_mode, int device);
+DDFAN_API void ddfan_plan_destroy(ddfan_plan* plan);
+/* device bytes held by the plan */
+DDFAN_API size_t ddfan_plan_device_bytes(const ddfan_plan* plan);
+
+/* Forward projection of device vol[YN][XN][SLN] into device prj[PN][DNU][SLN].
+ * d_angs: device view angles; angs_per_slice = 0: d_angs[PN] shared by all
+ * slices; 1: d_angs[PN][SLN] (the reference's hangs layout; slices whose
+ * angle lists differ are projected one group at a time).  Asynchronous on
+ * `stream` (a cudaStream_t, NULL = legacy default stream). */
+DDFAN_API int ddfan_proj_dev(ddfan_plan* plan, const float* d_angs, int PN, int angs_per_slice,
+                             const float* d_vol, float* d_prj, void* stream);
+/* Backprojection of device prj[PN][DNU][SLN] into device vol[YN][XN][SLN]. */
+DDFAN_API int ddfan_back_dev(ddfan_plan* plan, const float* d_angs, int PN, int angs_per_slice,
+                             const float* d_prj, float* d_vol, int back_mode, void* stream);
+
+/* ---- OS-SART / FISTA solver with device-resident state ----
+ * Replaces AAPM_script/OSSART_AAPM.m:33-118.  Subset k holds views
+ * k, k + numOfOS, ... (:60); row/column sums come from slice 0 (:61-64);
+ * where a sum is 0 the value is left un-normalised (:88, :94); FISTA momentum
+ * after each iteration (:111-115).  nonneg != 0 clamps the image at 0 after
+ * every subset update (an addition).  Each iteration is one CUDA graph. */
+typedef struct ddfan_ossart_s ddfan_ossart;
+
+DDFAN_API int ddfan_ossart_create(ddfan_ossart** out, float x0, float y0, int DNU,
+                                  const float* xds, const float* yds, float detCntIdx,
+                                  float imgXCenter, float imgYCenter, const float* hangs,
+                                  int PNall, int XN, int YN, int SLN, float dx,
+                                  const uint8_t* mask, int numOfOS, int useFISTA, int nonneg,
+                                  int sat_mode, int back_mode, int device);
+DDFAN_API void ddfan_ossart_destroy(ddfan_ossart* s);
+DDFAN_API size_t ddfan_ossart_device_bytes(const ddfan_ossart* s);
+/* measured sinogram proj[PNall][DNU][SLN]: host (to_device = 0 -> copied in
+ * with cudaMemcpyAsync) or device pointer (is_device = 1 -> copied D2D). */
+DDFAN_API int ddfan_ossart_set_sinogram(ddfan_ossart* s, const float* proj, int is_device,
+                                        void* stream);
+/* initial image [YN][XN][SLN], host or device; resets the FISTA state. */
+DDFAN_API int ddfan_ossart_set_image(ddfan_ossart* s, const float* img, int is_device,
+                                     void* stream);
+/* run numOfIter iterations on `stream` (graph per iteration when use_graph != 0) */
+DDFAN_API int ddfan_ossart_iterate(ddfan_ossart* s, int numOfIter, int use_graph, void* stream);
+/* copy the current image out (host or device destination) */
+DDFAN_API int ddfan_ossart_get_image(ddfan_ossart* s, float* img, int is_device, void* stream);
+/* device pointer of the current image (valid until the solver is destroyed) */
+DDFAN_API float* ddfan_ossart_image_ptr(ddfan_ossart* s);
+/* number of kernel launches one iteration issues */
+DDFAN_API int ddfan_ossart_launches_per_iter(const ddfan_ossart* s);
+
+/* One-call host entry mirroring OSSART_AAPM(Proj, Views, initImg, conf,
+ * numOfIter, numOfOS, mask, useFISTA) with the geometry already expanded. */
+DDFAN_API int ddfan_OSSART_AAPM(float x0, float y0, int DNU, const float* xds, const float* yds,
+                                float detCntIdx, float imgXCenter, float imgYCenter,
+                                const float* proj, const float* hangs, int PNall, int XN, int YN,
+                                int SLN, float dx, const float* initImg, const uint8_t* mask,
+                                int numOfIter, int numOfOS, int useFISTA, int nonneg,
+                                int sat_mode, int back_mode, float* reconImg);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DDFAN_H */
