@@ -44,6 +44,7 @@ SIGNATURES = {
     "ddfan_ossart_get_image": (_i, [_p, _p, _i, _p]),
     "ddfan_ossart_image_ptr": (_p, [_p]),
     "ddfan_ossart_launches_per_iter": (_i, [_p]),
+    "ddfan_ossart_profile": (_i, [_p, _i, _p, _p, _p]),
     "ddfan_OSSART_AAPM": (_i, [_f, _f, _i, _p, _p, _f, _f, _f, _p, _p, _i, _i, _i, _i, _f, _p, _p, _i,
                                _i, _i, _i, _i, _i, _p]),
 }

@@ -33,6 +33,34 @@ int set_err(int code, const char* fmt, ...) {
 
 const char* last_error() { return g_err.c_str(); }
 
+// ------------------------------------------------------------------ profiler
+
+LaunchProfiler*& active_profiler() {
+  static thread_local LaunchProfiler* p = nullptr;
+  return p;
+}
+
+int LaunchProfiler::mark(int k, cudaStream_t st) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+    if (a) cudaEventDestroy(a);
+    cudaGetLastError();
+    return -1;
+  }
+  cudaEventRecord(a, st);
+  ev.push_back(a);
+  ev.push_back(b);
+  kind.push_back(k);
+  return (int)kind.size() - 1;
+}
+
+void LaunchProfiler::done(int slot, cudaStream_t st) { cudaEventRecord(ev[2 * slot + 1], st); }
+
+LaunchProfiler::~LaunchProfiler() {
+  for (cudaEvent_t e : ev)
+    if (e) cudaEventDestroy(e);
+}
+
 // ------------------------------------------------------------------ plan
 
 static int pow2_zl(int ZB) {
@@ -211,6 +239,7 @@ static GeomConsts geom_consts(const Plan& p) {
 int launch_view_geom(const Plan& p, const float* d_angs, int stride, int PN, ViewGeom* vg,
                      double2* fc, float* cvd, cudaStream_t st) {
   if (PN < 1) return set_err(DDFAN_ERR_ARG, "PN must be >= 1");
+  ProfScope ps(KIND_VIEW_GEOM, st);
   k_view_geom<<<PN, 128, 0, st>>>(geom_consts(p), d_angs, stride, PN, vg, fc, cvd);
   return check_launch("k_view_geom");
 }
@@ -245,6 +274,7 @@ int launch_sat_image(const Plan& p, const float* d_vol, cudaStream_t st) {
   SatSrc s{};
   s.kind = 0; s.a = d_vol; s.mask = p.has_mask ? p.d_mask : nullptr;
   s.XN = p.XN; s.YN = p.YN; s.U = p.U; s.Z = p.Z;
+  ProfScope ps(KIND_SAT_IMAGE, st);
   return sat_launch(p.mode, s, p.d_satx, p.YN, p.d_saty, p.XN, p.XN, p.YN, p.XN, p.YN, p.ZB, 2, st);
 }
 
@@ -253,6 +283,7 @@ int launch_sat_sino(const Plan& p, const float* d_prj, int PN, const float* wgt,
   SatSrc s{};
   s.kind = 2; s.a = d_prj; s.wgt = wgt; s.wscale = wscale; s.y = y; s.yview = yview;
   s.rowsum = rowsum; s.XN = p.XN; s.YN = p.YN; s.U = p.U; s.Z = p.Z;
+  ProfScope ps(KIND_SAT_SINO, st);
   return sat_launch(p.mode, s, p.d_satq, PN, nullptr, 0, p.U, 0, p.U + 1, 0, p.ZB, 1, st);
 }
 
@@ -283,6 +314,7 @@ int launch_fwd(const Plan& p, const ViewGeom* vg, const double2* fc, const float
   a.satx = p.d_satx; a.saty = p.d_saty; a.vg = vg; a.fc = fc; a.cvd = cvd; a.order = order;
   a.out = d_prj; a.PN = PN; a.U = p.U; a.Z = p.Z; a.ZB = p.ZB; a.XN = p.XN; a.YN = p.YN;
   a.dx = p.dx; a.zlo = zlo; a.zhi = zhi;
+  ProfScope ps(KIND_FWD, st);
   switch (p.mode) {
     case SAT_FP32: fwd_zl<SAT_FP32>(p.ZL, a, st); break;
     case SAT_HILO: fwd_zl<SAT_HILO>(p.ZL, a, st); break;
@@ -339,6 +371,7 @@ int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2*
     a.XN = p.XN; a.YN = p.YN; a.ocx = p.ocx; a.ocy = p.ocy; a.dx = p.dx;
     a.inv_sid = p.inv_sid; a.inv_dbeta = p.inv_dbeta; a.cnt = (double)p.detCntIdx + 0.5;
     a.epi = epi;
+    ProfScope ps(KIND_BACK_A, st);
     switch (p.mode) {
       case SAT_FP32: ref_zl<SAT_FP32>(p.ZL, a, st); break;
       case SAT_HILO: ref_zl<SAT_HILO>(p.ZL, a, st); break;
@@ -357,20 +390,26 @@ int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2*
   a.epi = epi;
   a.epi.out = p.d_tmp; a.epi.addend = nullptr; a.epi.xin = nullptr; a.epi.colsum = nullptr;
   a.epi.nonneg = 0;
-  switch (p.mode) {
-    case SAT_FP32: adj_zl<SAT_FP32, true>(p.ZL, a, st); break;
-    case SAT_HILO: adj_zl<SAT_HILO, true>(p.ZL, a, st); break;
-    default: adj_zl<SAT_FP64, true>(p.ZL, a, st); break;
+  {
+    ProfScope ps(KIND_BACK_A, st);
+    switch (p.mode) {
+      case SAT_FP32: adj_zl<SAT_FP32, true>(p.ZL, a, st); break;
+      case SAT_HILO: adj_zl<SAT_HILO, true>(p.ZL, a, st); break;
+      default: adj_zl<SAT_FP64, true>(p.ZL, a, st); break;
+    }
   }
   int rc = check_launch("k_back_adj<x>");
   if (rc) return rc;
   // pass 2: y-major views, lines = y rows, plus pass 1, then the final epilogue
   a.epi = epi;
   a.epi.addend = p.d_tmp;
-  switch (p.mode) {
-    case SAT_FP32: adj_zl<SAT_FP32, false>(p.ZL, a, st); break;
-    case SAT_HILO: adj_zl<SAT_HILO, false>(p.ZL, a, st); break;
-    default: adj_zl<SAT_FP64, false>(p.ZL, a, st); break;
+  {
+    ProfScope ps(KIND_BACK_B, st);
+    switch (p.mode) {
+      case SAT_FP32: adj_zl<SAT_FP32, false>(p.ZL, a, st); break;
+      case SAT_HILO: adj_zl<SAT_HILO, false>(p.ZL, a, st); break;
+      default: adj_zl<SAT_FP64, false>(p.ZL, a, st); break;
+    }
   }
   return check_launch("k_back_adj<y>");
 }

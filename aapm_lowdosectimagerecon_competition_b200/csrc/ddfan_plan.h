@@ -71,6 +71,34 @@ int proj_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const floa
 int back_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const float* d_prj,
                     float* d_vol, int back_mode, int zlo, int zhi, cudaStream_t st);
 
+// Optional per-launch CUDA-event profiler: when active on the calling thread,
+// every kernel launch of the library is bracketed by two events on its stream.
+enum LaunchKind {
+  KIND_VIEW_GEOM = 0, KIND_SAT_IMAGE, KIND_FWD, KIND_SAT_SINO, KIND_BACK_A, KIND_BACK_B, KIND_FISTA,
+  KIND_COUNT
+};
+struct LaunchProfiler {
+  std::vector<cudaEvent_t> ev;  // pairs: before, after
+  std::vector<int> kind;
+  int mark(int k, cudaStream_t st);   // records the "before" event, returns the slot
+  void done(int slot, cudaStream_t st);
+  ~LaunchProfiler();
+};
+LaunchProfiler*& active_profiler();
+
+// Brackets one launch with profiler events when a profiler is active.
+struct ProfScope {
+  LaunchProfiler* p;
+  cudaStream_t st;
+  int slot = -1;
+  ProfScope(int kind, cudaStream_t s) : p(active_profiler()), st(s) {
+    if (p) slot = p->mark(kind, st);
+  }
+  ~ProfScope() {
+    if (p && slot >= 0) p->done(slot, st);
+  }
+};
+
 // Makes `dev` current for the scope and restores the caller's device.
 struct DeviceGuard {
   int prev = -1;

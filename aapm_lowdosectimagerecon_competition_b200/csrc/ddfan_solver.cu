@@ -245,6 +245,7 @@ static int solver_iteration(Solver& s, cudaStream_t st) {
   if (s.useFISTA) {
     const size_t V = (size_t)s.XN * s.YN * s.Z;
     const int blocks = (int)std::min<size_t>((V + 255) / 256, 148 * 16);
+    ProfScope ps(KIND_FISTA, st);
     k_fista<<<blocks, 256, 0, st>>>(s.d_x, s.d_xprev, V, s.d_t);
     k_fista_t<<<1, 1, 0, st>>>(s.d_t);
     cudaError_t e = cudaGetLastError();
@@ -476,6 +477,32 @@ DDFAN_API int ddfan_ossart_get_image(ddfan_ossart* h, float* img, int is_device,
   DDFAN_CK(cudaMemcpyAsync(img, s->d_x, sizeof(float) * n,
                            is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
   if (!is_device) DDFAN_CK(cudaStreamSynchronize(st));
+  return DDFAN_OK;
+}
+
+DDFAN_API int ddfan_ossart_profile(ddfan_ossart* h, int numOfIter, void* stream, float* ms_by_kind,
+                                   int* launches_by_kind) {
+  Solver* s = reinterpret_cast<Solver*>(h);
+  if (!s || numOfIter < 1 || !ms_by_kind || !launches_by_kind) return set_err(DDFAN_ERR_ARG, "bad argument");
+  DeviceGuard g(s->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  LaunchProfiler prof;
+  active_profiler() = &prof;
+  int rc = DDFAN_OK;
+  for (int it = 0; it < numOfIter && !rc; ++it) rc = solver_iteration(*s, st);
+  active_profiler() = nullptr;
+  if (rc) return rc;
+  DDFAN_CK(cudaStreamSynchronize(st));
+  for (int k = 0; k < KIND_COUNT; ++k) {
+    ms_by_kind[k] = 0.f;
+    launches_by_kind[k] = 0;
+  }
+  for (size_t i = 0; i < prof.kind.size(); ++i) {
+    float ms = 0.f;
+    DDFAN_CK(cudaEventElapsedTime(&ms, prof.ev[2 * i], prof.ev[2 * i + 1]));
+    ms_by_kind[prof.kind[i]] += ms;
+    launches_by_kind[prof.kind[i]] += prof.kind[i] == KIND_FISTA ? 2 : 1;
+  }
   return DDFAN_OK;
 }
 

@@ -140,6 +140,15 @@ class OSSART:
         call("ddfan_ossart_get_image", self._h, ptr, 0, _stream(stream))
         return out
 
+    KINDS = ("view_geom", "sat_image", "fwd", "sat_sino", "back_a", "back_b", "fista")
+
+    def profile(self, n=1, stream=None):
+        """Device ms and launch count per kernel kind over n ungraphed iterations."""
+        ms = (ctypes.c_float * 7)()
+        cnt = (ctypes.c_int * 7)()
+        call("ddfan_ossart_profile", self._h, int(n), _stream(stream), ms, cnt)
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(self.KINDS)}
+
     def close(self):
         if getattr(self, "_h", None):
             load().ddfan_ossart_destroy(self._h)

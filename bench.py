@@ -1,0 +1,380 @@
+"""Benchmark: OS-SART iterations/s on the full-reconstruction workload.
+
+Workload (one GPU, or one independent instance per rank): 512 x 512 x 128
+slices at 0.7 mm, 2304 views over 360 deg, 736 arc channels at 1.2858 mm,
+sid 595 mm, sdd 1085.6 mm, 24 ordered subsets, FISTA momentum and
+non-negativity, compensated hi/lo prefix sums, exact-adjoint backprojector;
+the sinogram is the log of seeded Poisson counts at I0 = 1.5e5 photons/ray of
+a seeded ellipsoid phantom (synthetic stand-in for the AAPM projections).
+A step is one OS-SART iteration (one CUDA graph replay, 24 subsets).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `--impl reference` times the FP64 CPU port of
+the reference path (oracle/) on this host's cores on a bounded sample of the
+same workload, scaled to the full image.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "OS-SART iters/s (512^2x128, 2304 views, 24 subsets)"
+UNIT = "iter/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--sat", default="hilo", choices=["fp32", "hilo", "fp64"])
+    ap.add_argument("--back", default="adj", choices=["ref", "adj"])
+    ap.add_argument("--slices", type=int, default=128)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    return ap.parse_args()
+
+
+def workload(slices):
+    from aapm_lowdosectimagerecon_competition_b200 import configs
+    return configs.c3(SLN=slices)
+
+
+def config_dict(s, args, n):
+    return {"workload": "OS-SART c3: %dx%dx%d, %d views, %d channels, %d subsets, FISTA+nonneg" %
+                        (s.XN, s.YN, s.SLN, s.PN, s.DNU, s.numOfOS),
+            "image": [s.XN, s.YN, s.SLN], "views": s.PN, "channels": s.DNU, "subsets": s.numOfOS,
+            "sat": args.sat, "back": args.back, "instances": n,
+            "l2": "inputs larger than L2 (sinogram 868 MB, image 134 MB, prefix-sum tables 0.8 GB)",
+            "parallelism": "one independent reconstruction per GPU (slices/requests shard with no exchange)"}
+
+
+# ----------------------------------------------------------------- CPU port
+
+def cpu_port_timing(s, slices, iters=1, nthreads=None):
+    """Seconds per OS-SART iteration of the FP64 CPU port on `slices` slices."""
+    from oracle import oracle as O
+    from oracle import np_oracle as N
+    x0, y0, xds, yds = N.fan_geometry(s.sid, s.sdd, s.DNU, s.detCellWidth, s.detCntIdx)
+    h = np.repeat(s.angles()[:, None], slices, 1)
+    y = np.zeros((s.PN, s.DNU, slices), np.float32)
+    init = np.zeros((s.YN, s.XN, slices), np.float32)
+    nt = nthreads or (os.cpu_count() or 1)
+    _, secs = O.ossart(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0.0, 0.0, h, s.PN, s.XN, s.YN, slices,
+                       y, init, s.dx, None, iters, s.numOfOS, s.useFISTA, s.nonneg,
+                       back_mode=O.ADJ, nthreads=nt, timing=True)
+    return secs / iters, nt
+
+
+def run_reference(args):
+    """--impl reference: the FP64 CPU port of the reference path (no CPU
+    implementation of the path exists in the reference itself)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    s = workload(args.slices)
+    sample = 2
+    from oracle import oracle as O
+    O.build()
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_port_timing(s, 1, 1)
+    per = []
+    nt = 1
+    for _ in range(args.steps):
+        sec, nt = cpu_port_timing(s, sample, 1)
+        per.append(sec * s.SLN / sample)
+    t = statistics.mean(per)
+    v = 1.0 / t
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config_dict(s, args, 1),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nt, "kind": "port",
+                             "sample": "1 OS-SART iteration (24 subsets, 2304 views) on %d of %d "
+                                       "slices per step, scaled by %d/%d (slices are independent)"
+                                       % (sample, s.SLN, s.SLN, sample)},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------- GPU arm
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for row in self.f.read().splitlines():
+            c = [x.strip() for x in row.split(",")]
+            if len(c) < 9:
+                continue
+            try:
+                sm.append(float(c[1]))
+                mx = float(c[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, c[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def make_problem(s, dev, seed=7):
+    """Phantom, noiseless sinogram (our forward), Poisson log sinogram; all on `dev`."""
+    import torch
+    from aapm_lowdosectimagerecon_competition_b200 import configs, dd2, device
+    x0, y0, xds, yds = dd2.fan_geometry(s.sid, s.sdd, s.DNU, s.detCellWidth, s.detCntIdx)
+    xt = torch.from_numpy(configs.phantom(s)).to(dev)
+    angs = torch.from_numpy(s.angles()).to(dev)
+    pl = device.Plan(x0, y0, s.DNU, xds, yds, s.detCntIdx, s.XN, s.YN, s.SLN, s.PN, s.dx,
+                     sat="fp64", device=dev.index)
+    prj = pl.proj(angs, xt)
+    pl.close()
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    counts = torch.poisson(s.I0 * torch.exp(-prj.double()), generator=g)
+    y = (-torch.log(torch.clamp(counts, min=1.0) / s.I0)).float()
+    torch.cuda.synchronize(dev)
+    return (x0, y0, xds, yds), xt, y
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from aapm_lowdosectimagerecon_competition_b200 import dd2, device
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    s = workload(args.slices)
+    (x0, y0, xds, yds), xt, y = make_problem(s, dev, seed=7 + rank)
+    mask = s.circular_mask()
+    solver = device.OSSART(x0, y0, s.DNU, xds, yds, s.detCntIdx, s.hangs(), s.XN, s.YN, s.SLN, s.dx,
+                           mask=mask, numOfOS=s.numOfOS, useFISTA=s.useFISTA, nonneg=s.nonneg,
+                           sat=args.sat, back=args.back, device=local)
+    solver.set_sinogram(y)
+    solver.set_image(torch.zeros_like(xt))
+    stream = torch.cuda.current_stream(dev)
+    solver.iterate(max(args.warmup, 3), use_graph=True, stream=stream)
+    torch.cuda.synchronize(dev)
+
+    # ---- timed region: K graph replays, device time on the launching stream
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    solver.iterate(args.steps, use_graph=True, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    ms_per_step = ms_max / args.steps
+    value = world * args.steps / (ms_max / 1e3)
+
+    # ---- per-kernel device time (events around every launch, same stream)
+    prof = solver.profile(1, stream=stream)
+    launches = solver.launches_per_iter * args.steps
+    top = max(("fwd", "back_a", "back_b", "sat_image", "sat_sino"), key=lambda k: prof[k][0])
+    V = s.XN * s.YN * s.SLN
+    S_sub = (s.PN // s.numOfOS) * s.DNU * s.SLN
+    # algorithmic bytes per launch (minimum HBM traffic): forward 4V + 4S,
+    # backprojection 4S + 4V (read the subset residual table once, write the image)
+    alg = {"fwd": 4.0 * (V + S_sub), "back_a": 4.0 * (V + S_sub), "back_b": 4.0 * (V + S_sub),
+           "sat_image": 4.0 * V + 2 * 12.0 * V, "sat_sino": 4.0 * S_sub + 12.0 * S_sub}
+    top_ms = prof[top][0] / max(prof[top][1], 1)
+    peak, peak_kind = peaks()
+    achieved = alg[top] / (top_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                "launch_ms": top_ms,
+                "kernel_ms_per_iter": {k: round(v[0], 3) for k, v in prof.items()},
+                "note": "achieved = algorithmic bytes per launch / CUDA-event launch time; the "
+                        "path is gather/issue bound, not HBM bound"}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config_dict(s, args, world), "gpu_launches": launches,
+            "clocks": clk, "roofline": roofline}
+
+    # ---- end to end through the public one-call API with host buffers
+    if not args.no_e2e:
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        y_h = pin(y.cpu().numpy())
+        x_h = pin(np.zeros((s.YN, s.XN, s.SLN), np.float32))
+        out_h = torch.empty((s.YN, s.XN, s.SLN), dtype=torch.float32).pin_memory()
+        conf = s.conf()
+        e2e_iters = 10
+        t_e2e = []
+        for rep in range(2):
+            torch.cuda.synchronize(dev)
+            if world > 1:
+                dist.barrier()
+            t0 = time.perf_counter()
+            _ossart_host(s, (x0, y0, xds, yds), y_h, x_h, out_h, mask, e2e_iters, args)
+            torch.cuda.synchronize(dev)
+            t_e2e.append(time.perf_counter() - t0)
+        te = min(t_e2e[1:] or t_e2e)
+        tt = torch.tensor([te], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        te = float(tt.item())
+        line["e2e"] = {"value": world * e2e_iters / te, "unit": UNIT,
+                       "h2d_bytes_per_step": int(y_h.numel() * 4 + x_h.numel() * 4 +
+                                                 s.PN * s.SLN * 4),
+                       "d2h_bytes_per_step": int(out_h.numel() * 4),
+                       "step": "one ddfan_OSSART_AAPM call: solver set-up, weights, %d iterations, "
+                               "pinned H2D of sinogram+image, D2H of the image" % e2e_iters,
+                       "seconds_per_call": te}
+
+    # ---- plain FP32 DD, one instance per launch, host round trips per subset
+    if not args.no_plain and rank == 0:
+        line["plain_fp32"] = plain_fp32_iteration(s, (x0, y0, xds, yds), y, mask)
+
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sample = 2
+        sec, nt = cpu_port_timing(s, sample, 1)
+        line["cpu_baseline"] = {"value": 1.0 / (sec * s.SLN / sample), "unit": UNIT, "cores": nt,
+                                "kind": "port",
+                                "sample": "1 OS-SART iteration (24 subsets, 2304 views, FP64, ADJ) on "
+                                          "%d of %d slices, scaled by %d/%d" % (sample, s.SLN, s.SLN,
+                                                                               sample)}
+    solver.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _ossart_host(s, geom, y_h, x_h, out_h, mask, iters, args):
+    import ctypes
+    from aapm_lowdosectimagerecon_competition_b200._lib import BACK_MODES, SAT_MODES, call
+    x0, y0, xds, yds = geom
+    hangs = np.ascontiguousarray(s.hangs())
+    m = np.ascontiguousarray(mask, np.uint8)
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    T = lambda t: ctypes.c_void_p(t.data_ptr())
+    call("ddfan_OSSART_AAPM", x0, y0, s.DNU, P(xds), P(yds), s.detCntIdx, 0.0, 0.0, T(y_h), P(hangs),
+         s.PN, s.XN, s.YN, s.SLN, s.dx, T(x_h), P(m), iters, s.numOfOS, s.useFISTA, s.nonneg,
+         SAT_MODES[args.sat], BACK_MODES[args.back], T(out_h))
+
+
+def plain_fp32_iteration(s, geom, y, mask):
+    """One OS-SART iteration executed the way AAPM_script/OSSART_AAPM.m drives
+    the mex functions: per subset a host-pointer projection call, the residual
+    on the host, a host-pointer backprojection call, the update on the host;
+    FP32 prefix sums, reference backprojector, no graphs."""
+    from aapm_lowdosectimagerecon_competition_b200 import dd2
+    x0, y0, xds, yds = geom
+    yh = y.cpu().numpy()
+    hangs = s.hangs()
+    x = np.zeros((s.YN, s.XN, s.SLN), np.float32)
+    ones_i = np.ones((s.YN, s.XN, 1), np.float32)
+    subs = [np.arange(k, s.PN, s.numOfOS) for k in range(s.numOfOS)]
+    rows, cols = [], []
+    for v in subs:
+        h1 = np.ascontiguousarray(hangs[v][:, :1])
+        rows.append(dd2.MultiSlicesProjGPU(x0, y0, s.DNU, xds, yds, 0, 0, h1, len(v), s.XN, s.YN, 1,
+                                           ones_i, s.dx, mask, sat="fp32"))
+        cols.append(dd2.MultiSlicesBackGPU(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0, 0, h1, len(v),
+                                           s.XN, s.YN, 1, np.ones((len(v), s.DNU, 1), np.float32), s.dx,
+                                           mask, sat="fp32", back="ref"))
+    t0 = time.perf_counter()
+    for k, v in enumerate(subs):
+        h = np.ascontiguousarray(hangs[v])
+        prj = dd2.MultiSlicesProjGPU(x0, y0, s.DNU, xds, yds, 0, 0, h, len(v), s.XN, s.YN, s.SLN, x,
+                                     s.dx, mask, sat="fp32")
+        rs = rows[k]
+        nz = np.broadcast_to(rs != 0, prj.shape)
+        prj = np.where(nz, (yh[v] - prj) / np.where(rs != 0, rs, 1), prj).astype(np.float32)
+        tp = dd2.MultiSlicesBackGPU(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0, 0, h, len(v), s.XN, s.YN,
+                                    s.SLN, prj, s.dx, mask, sat="fp32", back="ref")
+        cs = cols[k]
+        tp = np.where(np.broadcast_to(cs != 0, tp.shape), tp / np.where(cs != 0, cs, 1), tp)
+        x = np.maximum(x + tp, 0).astype(np.float32)
+    sec = time.perf_counter() - t0
+    return {"value": 1.0 / sec, "unit": UNIT, "seconds_per_iter": sec,
+            "how": "mex-style: per subset host->device image, FP32 prefix sums, forward, "
+                   "device->host sinogram, host residual, host->device, REF backprojection, "
+                   "device->host image, host update (AAPM_script/OSSART_AAPM.m:79-97); no graphs"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -142,6 +142,14 @@ DDFAN_API int ddfan_ossart_iterate(ddfan_ossart* s, int numOfIter, int use_graph
 DDFAN_API int ddfan_ossart_get_image(ddfan_ossart* s, float* img, int is_device, void* stream);
 /* device pointer of the current image (valid until the solver is destroyed) */
 DDFAN_API float* ddfan_ossart_image_ptr(ddfan_ossart* s);
+/* Runs numOfIter iterations without a graph, each kernel launch bracketed by
+ * CUDA events on `stream`; returns per kind the summed device milliseconds
+ * and launch counts.  Kinds: 0 view geometry, 1 image prefix sums,
+ * 2 forward projection, 3 sinogram prefix sums (+ residual), 4 backprojection
+ * (REF, or exact-adjoint column pass), 5 exact-adjoint row pass, 6 FISTA.
+ * Arrays must hold 7 entries.  (Diagnostics; no counterpart in the reference.) */
+DDFAN_API int ddfan_ossart_profile(ddfan_ossart* s, int numOfIter, void* stream, float* ms_by_kind,
+                                   int* launches_by_kind);
 /* number of kernel launches one iteration issues */
 DDFAN_API int ddfan_ossart_launches_per_iter(const ddfan_ossart* s);
 

@@ -431,12 +431,13 @@ int orc_back_d(float x0, float y0, int DNU, const float* xds, const float* yds, 
  * Row/column sums come from slice 0 and are reused for every slice (:61-64).
  * Where a row/column sum is 0 the value is left un-normalised (:88, :94).
  * nonneg != 0 clamps the image at 0 after every subset update (not in the
- * reference).  back_mode: 0 REF, 1 ADJ. */
+ * reference).  back_mode: 0 REF, 1 ADJ.  *iter_seconds (may be NULL) gets the
+ * wall time of the iterations alone (weights excluded). */
 int orc_ossart(float x0, float y0, int DNU, const float* xds, const float* yds, float detCntIdx,
                float imgXCenter, float imgYCenter, const float* hangs, int PNall, int XN, int YN,
                int SLN, const float* proj, const float* init, float dx, const uint8_t* mask,
                int numOfIter, int numOfOS, int useFISTA, int nonneg, int back_mode, double* out,
-               int nthreads) {
+               int nthreads, double* iter_seconds) {
   geom_t g;
   if (numOfOS < 1 || numOfOS > PNall) return -2;
   if (geom_init(&g, x0, y0, DNU, xds, yds, imgXCenter, imgYCenter, XN, YN, dx, mask)) return -1;
@@ -467,6 +468,10 @@ int orc_ossart(float x0, float y0, int DNU, const float* xds, const float* yds, 
     if (rc) goto done;
   }
   double t0 = 1.0;
+  double wall0 = 0.0;
+#ifdef _OPENMP
+  wall0 = omp_get_wtime();
+#endif
   for (int it = 0; it < numOfIter; ++it) {
     if (useFISTA) memcpy(last, x, sizeof(double) * V);
     for (int k = 0; k < numOfOS; ++k) {
@@ -504,6 +509,13 @@ int orc_ossart(float x0, float y0, int DNU, const float* xds, const float* yds, 
       for (size_t e = 0; e < V; ++e) x[e] = x[e] + m * (x[e] - last[e]);
       t0 = t1;
     }
+  }
+  if (iter_seconds) {
+#ifdef _OPENMP
+    *iter_seconds = omp_get_wtime() - wall0;
+#else
+    *iter_seconds = 0.0;
+#endif
   }
 done:
   free(last); free(angs); free(angs1); free(ysub); free(prj); free(tp); free(rows); free(cols);

@@ -46,7 +46,7 @@ def lib():
         L.orc_proj_d.argtypes = L.orc_proj.argtypes
         L.orc_back_d.argtypes = L.orc_back.argtypes
         L.orc_ossart.argtypes = [_f, _f, _i, _p, _p, _f, _f, _f, _p, _i, _i, _i, _i, _p, _p, _f,
-                                 _p, _i, _i, _i, _i, _i, _p, _i]
+                                 _p, _i, _i, _i, _i, _i, _p, _i, _p]
         L.orc_boundaries.argtypes = [_i, _p, _p]
         for fn in (L.orc_proj, L.orc_back, L.orc_proj_d, L.orc_back_d, L.orc_ossart):
             fn.restype = _i
@@ -126,17 +126,19 @@ def back(x0, y0, DNU, xds, yds, detCntIdx, imgXCenter, imgYCenter, hangs, PN, XN
 
 def ossart(x0, y0, DNU, xds, yds, detCntIdx, imgXCenter, imgYCenter, hangs, PNall, XN, YN, SLN,
            proj_meas, init, dx, mask, numOfIter, numOfOS, useFISTA=1, nonneg=0, back_mode=REF,
-           nthreads=None):
-    """FP64 OS-SART (+FISTA, optional non-negativity) -> float64 [YN][XN][SLN]."""
+           nthreads=None, timing=False):
+    """FP64 OS-SART (+FISTA, optional non-negativity) -> float64 [YN][XN][SLN]
+    (and the iterations' wall time in seconds when timing=True)."""
     xds = _c(xds, np.float32); yds = _c(yds, np.float32)
     a = _c(hangs, np.float32); y = _c(proj_meas, np.float32); x0i = _c(init, np.float32)
     m = _mask(mask, XN, YN)
     out = np.zeros((YN, XN, SLN), np.float64)
     nt = nthreads or nthreads_default()
+    secs = ctypes.c_double(0.0)
     rc = lib().orc_ossart(x0, y0, DNU, _ptr(xds), _ptr(yds), detCntIdx, imgXCenter, imgYCenter,
                           _ptr(a), PNall, XN, YN, SLN, _ptr(y), _ptr(x0i), dx, _ptr(m),
                           numOfIter, numOfOS, int(useFISTA), int(nonneg), int(back_mode),
-                          _ptr(out), nt)
+                          _ptr(out), nt, ctypes.byref(secs))
     if rc:
         raise RuntimeError("orc_ossart failed (%d)" % rc)
-    return out
+    return (out, secs.value) if timing else out

@@ -1,0 +1,232 @@
+"""Parity of the sm_100a kernels (through the C ABI) with the FP64 oracle and
+with the reference's own kernels.  Needs a B200.
+
+Tolerances (relative L2 against the FP64 oracle):
+  compensated hi/lo or FP64 prefix sums: 2e-6 per projection/backprojection,
+  1e-5 on an OS-SART image; plain FP32 prefix sums: 5e-5 at these sizes.
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def rel(a, b):
+    return float(np.linalg.norm((np.asarray(a, np.float64) - b).ravel()) / np.linalg.norm(np.ravel(b)))
+
+
+TOL = {"fp32": 5e-5, "hilo": 2e-6, "fp64": 2e-6}
+
+
+@pytest.fixture(scope="module")
+def mods():
+    import torch
+    assert torch.cuda.is_available()
+    from aapm_lowdosectimagerecon_competition_b200 import configs, dd2, device
+    from oracle import oracle as O
+    return dd2, configs, device, O
+
+
+def make_case(configs, dd2, XN=40, YN=40, SLN=8, PN=60, DNU=72, cx=0.0, cy=0.0, dcnt=0.0,
+              per_slice=False, masked=False, seed=0):
+    s = configs.scaled(configs.c2(SLN=SLN), XN=XN, DNU=DNU, PN=PN)
+    s.YN = YN
+    s.detCntIdx += dcnt
+    x0, y0, xds, yds = dd2.fan_geometry(s.sid, s.sdd, s.DNU, s.detCellWidth, s.detCntIdx)
+    rng = np.random.default_rng(seed)
+    h = s.hangs()
+    if per_slice:
+        h = (h + rng.uniform(0, 2 * math.pi, SLN)[None, :]).astype(np.float32)
+    vol = (rng.random((YN, XN, SLN)) * 0.03).astype(np.float32)
+    mask = None
+    if masked:
+        yy, xx = np.meshgrid(np.arange(YN) - YN / 2, np.arange(XN) - XN / 2, indexing="ij")
+        mask = ((xx / (0.5 * XN)) ** 2 + (yy / (0.5 * YN)) ** 2 < 0.8).astype(np.uint8)
+    prj = rng.random((PN, DNU, SLN)).astype(np.float32)
+    geo = dict(x0=x0, y0=y0, DNU=DNU, xds=xds, yds=yds, cnt=np.float32(s.detCntIdx),
+               cx=np.float32(cx), cy=np.float32(cy), h=h, PN=PN, XN=XN, YN=YN, SLN=SLN,
+               dx=np.float32(s.dx), mask=mask)
+    return geo, vol, prj
+
+
+CASES = {
+    "square": dict(),
+    "rect_offcentre_quarter": dict(XN=36, YN=28, cx=3.5, cy=-2.0, dcnt=0.25),
+    "masked_perslice": dict(SLN=5, per_slice=True, masked=True),
+    "single_slice": dict(SLN=1),
+    "odd_slices": dict(SLN=13, XN=24, YN=30),
+    "many_slices": dict(SLN=64, XN=32, YN=32, PN=30),
+}
+
+
+def fwd(dd2, g, vol, sat):
+    return dd2.MultiSlicesProjGPU(g["x0"], g["y0"], g["DNU"], g["xds"], g["yds"], g["cx"], g["cy"], g["h"],
+                                  g["PN"], g["XN"], g["YN"], g["SLN"], vol, g["dx"], g["mask"], sat=sat)
+
+
+def bwd(dd2, g, prj, sat, back):
+    return dd2.MultiSlicesBackGPU(g["x0"], g["y0"], g["DNU"], g["xds"], g["yds"], g["cnt"], g["cx"], g["cy"],
+                                  g["h"], g["PN"], g["XN"], g["YN"], g["SLN"], prj, g["dx"], g["mask"],
+                                  sat=sat, back=back)
+
+
+def ofwd(O, g, vol):
+    return O.proj(g["x0"], g["y0"], g["DNU"], g["xds"], g["yds"], g["cx"], g["cy"], g["h"], g["PN"],
+                  g["XN"], g["YN"], g["SLN"], vol, g["dx"], g["mask"])
+
+
+def obwd(O, g, prj, mode):
+    return O.back(g["x0"], g["y0"], g["DNU"], g["xds"], g["yds"], g["cnt"], g["cx"], g["cy"], g["h"],
+                  g["PN"], g["XN"], g["YN"], g["SLN"], prj, g["dx"], g["mask"], mode=mode)
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+@pytest.mark.parametrize("sat", ["fp32", "hilo", "fp64"])
+def test_forward_matches_oracle(mods, case, sat):
+    dd2, configs, device, O = mods
+    g, vol, _ = make_case(configs, dd2, **CASES[case])
+    assert rel(fwd(dd2, g, vol, sat), ofwd(O, g, vol)) < TOL[sat]
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+@pytest.mark.parametrize("sat", ["fp32", "hilo", "fp64"])
+@pytest.mark.parametrize("back", ["ref", "adj"])
+def test_backprojection_matches_oracle(mods, case, sat, back):
+    dd2, configs, device, O = mods
+    g, _, prj = make_case(configs, dd2, **CASES[case])
+    out = bwd(dd2, g, prj, sat, back)
+    exp = obwd(O, g, prj, O.REF if back == "ref" else O.ADJ)
+    assert rel(out, exp) < TOL[sat]
+    if g["mask"] is not None:
+        assert np.all(out[g["mask"] == 0] == 0)
+
+
+@pytest.mark.parametrize("sat", ["hilo", "fp64"])
+def test_adjoint_identity_on_gpu(mods, sat):
+    dd2, configs, device, O = mods
+    g, vol, prj = make_case(configs, dd2, XN=48, YN=40, SLN=8, PN=90, DNU=96, masked=True)
+    Ax = fwd(dd2, g, vol, sat).astype(np.float64)
+    ATy = bwd(dd2, g, prj, sat, "adj").astype(np.float64)
+    lhs, rhs = float((Ax * prj).sum()), float((vol * ATy).sum())
+    assert abs(lhs - rhs) / abs(lhs) < 1e-6
+
+
+def fixture_cases():
+    f = np.load(os.path.join(HERE, "golden", "ref_fixtures.npz"))
+    names = sorted({k.split("/")[0] for k in f.files})
+    return [(n, {k.split("/", 1)[1]: f[k] for k in f.files if k.startswith(n + "/")}) for n in names]
+
+
+@pytest.mark.parametrize("name,c", fixture_cases())
+def test_ref_mode_matches_reference_kernels(mods, name, c):
+    """Drop-in parity with the reference's own kernels (texture precision)."""
+    dd2 = mods[0]
+    a = (c["x0"], c["y0"], int(c["DNU"]), c["xds"], c["yds"])
+    geo = (c["hangs"], int(c["PN"]), int(c["XN"]), int(c["YN"]), int(c["SLN"]))
+    P = dd2.MultiSlicesProjGPU(*a, c["imgXCenter"], c["imgYCenter"], *geo, c["vol"], c["dx"], c["mask"])
+    assert rel(P, c["ref_proj"]) < 2e-3
+    B = dd2.MultiSlicesBackGPU(*a, c["detCntIdx"], c["imgXCenter"], c["imgYCenter"], *geo, c["prj_in"],
+                               c["dx"], c["mask"], back="ref")
+    assert rel(B, c["ref_back"]) < 2e-3
+
+
+def test_start_idx_slabs_match_single_slab(mods):
+    dd2, configs, device, O = mods
+    g, vol, prj = make_case(configs, dd2, SLN=11, per_slice=True)
+    one = fwd(dd2, g, vol, "hilo")
+    args = (g["x0"], g["y0"], g["DNU"], g["xds"], g["yds"], g["cx"], g["cy"], g["h"], g["PN"], g["XN"],
+            g["YN"], g["SLN"], vol, g["dx"], g["mask"])
+    slabs = dd2.MultiSlicesProjGPU(*args, startIdx=[0, 4, 4, 9], sat="hilo")
+    np.testing.assert_allclose(slabs, one, rtol=1e-6, atol=1e-7)
+    b1 = bwd(dd2, g, prj, "hilo", "adj")
+    bs = dd2.MultiSlicesBackGPU(g["x0"], g["y0"], g["DNU"], g["xds"], g["yds"], g["cnt"], g["cx"], g["cy"],
+                                g["h"], g["PN"], g["XN"], g["YN"], g["SLN"], prj, g["dx"], g["mask"],
+                                startIdx=dd2.default_start_idx(g["SLN"], 3), back="adj")
+    np.testing.assert_allclose(bs, b1, rtol=1e-6, atol=1e-7)
+    with pytest.raises(Exception):
+        dd2.MultiSlicesProjGPU(*args, startIdx=[1, 4])
+
+
+def test_device_api_matches_host_api(mods):
+    import torch
+    dd2, configs, device, O = mods
+    g, vol, prj = make_case(configs, dd2, SLN=12)
+    pl = device.Plan(g["x0"], g["y0"], g["DNU"], g["xds"], g["yds"], g["cnt"], g["XN"], g["YN"], g["SLN"],
+                     g["PN"], g["dx"], sat="hilo")
+    angs = torch.from_numpy(np.ascontiguousarray(g["h"][:, 0])).cuda()
+    p_dev = pl.proj(angs, torch.from_numpy(vol).cuda()).cpu().numpy()
+    np.testing.assert_allclose(p_dev, fwd(dd2, g, vol, "hilo"), rtol=1e-6, atol=1e-7)
+    for back in ("ref", "adj"):
+        b_dev = pl.back(angs, torch.from_numpy(prj).cuda(), mode=back).cpu().numpy()
+        np.testing.assert_allclose(b_dev, bwd(dd2, g, prj, "hilo", back), rtol=1e-6, atol=1e-7)
+    # per-slice angle tensor (PN, SLN) takes the grouped path
+    hp = torch.from_numpy(np.ascontiguousarray(g["h"])).cuda()
+    np.testing.assert_allclose(pl.proj(hp, torch.from_numpy(vol).cuda()).cpu().numpy(), p_dev,
+                               rtol=1e-6, atol=1e-7)
+    pl.close()
+
+
+def solver_case(configs, dd2, O, SLN=6, XN=40, PN=96, DNU=64, nsub=6):
+    s = configs.scaled(configs.c3(SLN=SLN), XN=XN, DNU=DNU, PN=PN)
+    s.numOfOS = nsub
+    x0, y0, xds, yds = dd2.fan_geometry(s.sid, s.sdd, s.DNU, s.detCellWidth, s.detCntIdx)
+    xt = configs.phantom(s)
+    mask = s.circular_mask()
+    y = O.proj(x0, y0, s.DNU, xds, yds, 0, 0, s.hangs(), s.PN, s.XN, s.YN, s.SLN, xt, s.dx, mask)
+    y = configs.poisson_log(y, 1.5e5, seed=5)
+    return s, (x0, y0, xds, yds), xt, mask, y
+
+
+@pytest.mark.parametrize("back", ["ref", "adj"])
+@pytest.mark.parametrize("nonneg", [0, 1])
+def test_ossart_matches_oracle(mods, back, nonneg):
+    dd2, configs, device, O = mods
+    s, (x0, y0, xds, yds), xt, mask, y = solver_case(configs, dd2, O)
+    init = np.zeros_like(xt)
+    xg = dd2.OSSART_AAPM(y, s.hangs(), init, s.conf(), 5, s.numOfOS, mask, 1, nonneg, sat="hilo", back=back)
+    xo = O.ossart(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0, 0, s.hangs(), s.PN, s.XN, s.YN, s.SLN, y, init,
+                  s.dx, mask, 5, s.numOfOS, 1, nonneg, O.REF if back == "ref" else O.ADJ)
+    assert rel(xg, xo) < 1e-5
+    if nonneg:
+        assert xg.min() >= 0
+
+
+def test_ossart_graph_equals_stream_launches(mods):
+    import torch
+    dd2, configs, device, O = mods
+    s, (x0, y0, xds, yds), xt, mask, y = solver_case(configs, dd2, O, SLN=8)
+    res = []
+    for graph in (True, False):
+        sv = device.OSSART(x0, y0, s.DNU, xds, yds, s.detCntIdx, s.hangs(), s.XN, s.YN, s.SLN, s.dx, mask=mask,
+                           numOfOS=s.numOfOS, useFISTA=1, nonneg=1, sat="hilo", back="adj")
+        sv.set_sinogram(torch.from_numpy(y).cuda())
+        sv.set_image(torch.zeros((s.YN, s.XN, s.SLN)).cuda())
+        sv.iterate(3, use_graph=graph)
+        torch.cuda.synchronize()
+        res.append(sv.image().cpu().numpy())
+        sv.close()
+    np.testing.assert_array_equal(res[0], res[1])
+
+
+def test_compensated_sums_beat_fp32_at_full_width(mods):
+    """512-pixel lines (config-2 geometry): plain FP32 prefix sums lose accuracy
+    in the difference of two large sums; hi/lo and FP64 keep ~1e-7."""
+    dd2, configs, device, O = mods
+    s = configs.c2(SLN=4)
+    x0, y0, xds, yds = dd2.fan_geometry(s.sid, s.sdd, s.DNU, s.detCellWidth, s.detCntIdx)
+    PN = 24
+    h = np.ascontiguousarray(s.hangs()[::96][:PN])
+    vol = configs.ellipsoid_phantom_3d(s)
+    exp = O.proj(x0, y0, s.DNU, xds, yds, 0, 0, h, PN, s.XN, s.YN, s.SLN, vol, s.dx)
+    err = {}
+    for sat in ("fp32", "hilo", "fp64"):
+        got = dd2.MultiSlicesProjGPU(x0, y0, s.DNU, xds, yds, 0, 0, h, PN, s.XN, s.YN, s.SLN, vol, s.dx,
+                                     sat=sat)
+        err[sat] = rel(got, exp)
+    assert err["hilo"] < 1e-6 and err["fp64"] < 1e-6
+    assert err["fp32"] > err["hilo"]
