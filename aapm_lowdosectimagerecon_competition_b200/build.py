@@ -11,7 +11,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libddfan.so")
 SOURCES = ["ddfan.cu", "ddfan_solver.cu"]
-HEADERS = ["ddfan_device.cuh", "ddfan_kernels.cuh", "ddfan_plan.h"]
+HEADERS = ["ddfan_device.cuh", "ddfan_kernels.cuh", "ddfan_proj_kernels.cuh", "ddfan_plan.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -19,7 +19,7 @@ def _stale():
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".h"))]
     deps.append(os.path.join(ROOT, "include", "ddfan.h"))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 

@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -63,11 +64,22 @@ LaunchProfiler::~LaunchProfiler() {
 
 // ------------------------------------------------------------------ plan
 
+// z-blocks per z-tile: wider tiles gather more contiguous bytes per request,
+// but a stack of ZB blocks is padded to whole tiles.  Relative cost per
+// padded block of each width (measured on the 512^2 x 128 workload: widths
+// 8, 4, 2 ran at 1 : 1.2 : 2.1); pick the cheapest padded stack.
 static int pow2_zl(int ZB) {
-  if (ZB >= 8) return 8;
-  if (ZB >= 4) return 4;
-  if (ZB >= 2) return 2;
-  return 1;
+  const int widths[4] = {8, 4, 2, 1};
+  const double cost[4] = {1.0, 1.2, 2.1, 3.6};
+  int best = 1;
+  double bc = 1e300;
+  for (int i = 0; i < 4; ++i) {
+    const int w = widths[i];
+    if (w > ZB) continue;
+    const double c = (double)((ZB + w - 1) / w * w) * cost[i];
+    if (c < bc) { bc = c; best = w; }
+  }
+  return best;
 }
 
 template <class T>
@@ -90,7 +102,8 @@ void plan_free(Plan* P) {
   cudaGetDevice(&prev);
   cudaSetDevice(P->device);
   void* ptrs[] = {P->d_bx, P->d_by, P->d_xd, P->d_yd, P->d_mask, P->d_tb, P->d_lut, P->d_satx,
-                  P->d_saty, P->d_satq, P->d_vg, P->d_fc, P->d_cvd, P->d_tmp, P->d_angs};
+                  P->d_saty, P->d_satq, P->d_vg, P->d_fc, P->d_cvd, P->d_tmp, P->d_angs,
+                  P->d_order, P->d_counts};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (prev >= 0) cudaSetDevice(prev);
@@ -139,6 +152,11 @@ int plan_create(Plan** out, const PlanDesc& d) {
   p.device = d.device;
   p.XN = d.XN; p.YN = d.YN; p.U = d.DNU; p.Z = d.SLN; p.ZB = (d.SLN + 3) / 4;
   p.PNmax = d.PNmax; p.mode = d.sat_mode; p.ZL = pow2_zl(p.ZB);
+  if (const char* zl = getenv("DDFAN_ZL")) {
+    const int v = atoi(zl);
+    if ((v == 1 || v == 2 || v == 4 || v == 8) && v <= p.ZL) p.ZL = v;
+  }
+  p.ZB = (p.ZB + p.ZL - 1) / p.ZL * p.ZL;  // whole z-tiles (padding blocks hold zeros)
   p.x0 = d.x0; p.y0 = d.y0; p.dx = d.dx; p.detCntIdx = d.detCntIdx;
   p.ocx = (d.XN - 1.0) * 0.5 - (double)d.imgXCenter / (double)d.dx;
   p.ocy = (d.YN - 1.0) * 0.5 - (double)d.imgYCenter / (double)d.dx;
@@ -197,7 +215,8 @@ int plan_create(Plan** out, const PlanDesc& d) {
       (rc = dalloc(&p.d_vg, p.PNmax, &B)) || (rc = dalloc(&p.d_fc, (size_t)p.PNmax * (p.U + 1), &B)) ||
       (rc = dalloc(&p.d_cvd, (size_t)p.PNmax * p.U, &B)) ||
       (rc = dalloc(&p.d_tmp, (size_t)p.XN * p.YN * p.Z, &B)) ||
-      (rc = dalloc(&p.d_angs, (size_t)p.PNmax, &B))) {
+      (rc = dalloc(&p.d_angs, (size_t)p.PNmax, &B)) ||
+      (rc = dalloc(&p.d_order, (size_t)p.PNmax, &B)) || (rc = dalloc(&p.d_counts, 2, &B))) {
     if (prev >= 0) cudaSetDevice(prev);
     return rc;
   }
@@ -273,7 +292,7 @@ static int sat_launch(int mode, const SatSrc& s, float4* out0, int nl0, float4* 
 int launch_sat_image(const Plan& p, const float* d_vol, cudaStream_t st) {
   SatSrc s{};
   s.kind = 0; s.a = d_vol; s.mask = p.has_mask ? p.d_mask : nullptr;
-  s.XN = p.XN; s.YN = p.YN; s.U = p.U; s.Z = p.Z;
+  s.XN = p.XN; s.YN = p.YN; s.U = p.U; s.Z = p.Z; s.ZLt = p.ZL;
   ProfScope ps(KIND_SAT_IMAGE, st);
   return sat_launch(p.mode, s, p.d_satx, p.YN, p.d_saty, p.XN, p.XN, p.YN, p.XN, p.YN, p.ZB, 2, st);
 }
@@ -282,19 +301,27 @@ int launch_sat_sino(const Plan& p, const float* d_prj, int PN, const float* wgt,
                     const float* y, const int* yview, const float* rowsum, cudaStream_t st) {
   SatSrc s{};
   s.kind = 2; s.a = d_prj; s.wgt = wgt; s.wscale = wscale; s.y = y; s.yview = yview;
-  s.rowsum = rowsum; s.XN = p.XN; s.YN = p.YN; s.U = p.U; s.Z = p.Z;
+  s.rowsum = rowsum; s.XN = p.XN; s.YN = p.YN; s.U = p.U; s.Z = p.Z; s.ZLt = p.ZL;
   ProfScope ps(KIND_SAT_SINO, st);
   return sat_launch(p.mode, s, p.d_satq, PN, nullptr, 0, p.U, 0, p.U + 1, 0, p.ZB, 1, st);
 }
 
-constexpr int FWD_CG = 8;
-constexpr int BACK_VG = 8;
+// Views of a call in dispatch order (x-major first) and their counts.
+int launch_view_order(const ViewGeom* vg, int PN, int* order, int* counts, cudaStream_t st) {
+  ProfScope ps(KIND_VIEW_GEOM, st);
+  k_view_order<<<1, 1024, 0, st>>>(vg, PN, order, counts);
+  return check_launch("k_view_order");
+}
+
+// channels per thread of the forward projector for a z-lane count
+template <int ZL> struct FwdCG { static constexpr int v = ZL >= 4 ? 4 : (ZL == 2 ? 2 : 1); };
 
 template <int M, int ZL>
 static void fwd_go(const FwdArgs& a, cudaStream_t st) {
-  constexpr int NG = 32 / ZL;
-  dim3 grid((a.U + 4 * NG * FWD_CG - 1) / (4 * NG * FWD_CG), a.PN, (a.ZB + ZL - 1) / ZL);
-  k_fwd<M, ZL, FWD_CG><<<grid, 128, 0, st>>>(a);
+  constexpr int CG = FwdCG<ZL>::v;
+  using T = FwdTile<ZL, CG>;
+  dim3 grid((a.U + T::CW - 1) / T::CW, a.PN, (a.ZB + ZL - 1) / ZL);
+  k_fwd<M, ZL, CG><<<grid, T::NT, 0, st>>>(a);
 }
 
 template <int M>
@@ -325,19 +352,19 @@ int launch_fwd(const Plan& p, const ViewGeom* vg, const double2* fc, const float
 
 template <int M, int ZL>
 static void ref_go(const RefArgs& a, cudaStream_t st) {
-  constexpr int NG = 32 / ZL;
-  const int nseg = (a.XN + BACK_VG - 1) / BACK_VG;
-  dim3 grid((nseg * a.YN + 4 * NG - 1) / (4 * NG), 1, (a.ZB + ZL - 1) / ZL);
-  k_back_ref<M, ZL, BACK_VG><<<grid, 128, 0, st>>>(a);
+  using T = BackTile<ZL>;
+  const int tiles = ((a.YN + T::LT - 1) / T::LT) * ((a.XN + T::KT - 1) / T::KT);
+  dim3 grid(tiles, 1, (a.ZB + ZL - 1) / ZL);
+  k_back_ref<M, ZL><<<grid, T::NT, 0, st>>>(a);
 }
 
 template <int M, int ZL, bool XM>
 static void adj_go(const AdjArgs& a, cudaStream_t st) {
-  constexpr int NG = 32 / ZL;
+  using T = BackTile<ZL>;
   const int nl = XM ? a.XN : a.YN, N = XM ? a.YN : a.XN;
-  const int nseg = (N + BACK_VG - 1) / BACK_VG;
-  dim3 grid((nseg * nl + 4 * NG - 1) / (4 * NG), 1, (a.ZB + ZL - 1) / ZL);
-  k_back_adj<M, ZL, BACK_VG, XM><<<grid, 128, 0, st>>>(a);
+  const int tiles = ((nl + T::LT - 1) / T::LT) * ((N + T::KT - 1) / T::KT);
+  dim3 grid(tiles, 1, (a.ZB + ZL - 1) / ZL);
+  k_back_adj<M, ZL, XM><<<grid, T::NT, 0, st>>>(a);
 }
 
 template <int M>
@@ -362,9 +389,10 @@ static void adj_zl(int ZL, const AdjArgs& a, cudaStream_t st) {
 
 // Backprojection of the table in p.d_satq (built by launch_sat_sino with the
 // matching weights).  `epi` holds the final destination/update; ADJ runs two
-// passes (x-column lines, then y-row lines) through p.d_tmp.
-int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2* fc, int PN,
-                const BackEpi& epi, cudaStream_t st) {
+// passes (x-column lines over the x-major views, then y-row lines over the
+// others) through p.d_tmp.  order/counts come from launch_view_order.
+int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2* fc,
+                const int* order, const int* counts, int PN, const BackEpi& epi, cudaStream_t st) {
   if (back_mode == DDFAN_BACK_REF) {
     RefArgs a;
     a.satq = p.d_satq; a.vg = vg; a.PN = PN; a.U = p.U; a.Z = p.Z; a.ZB = p.ZB;
@@ -381,8 +409,10 @@ int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2*
   }
   if (back_mode != DDFAN_BACK_ADJ) return set_err(DDFAN_ERR_ARG, "back_mode %d", back_mode);
   if (!p.adj_ok) return set_err(DDFAN_ERR_UNSUPPORTED, "detector boundaries are not monotone as seen from the source");
+  if (!order || !counts) return set_err(DDFAN_ERR_ARG, "exact adjoint needs the view order");
   AdjArgs a;
   a.satq = p.d_satq; a.vg = vg; a.fc = fc; a.tb = p.d_tb; a.lut = p.d_lut;
+  a.order = order; a.counts = counts;
   a.t0 = p.t0; a.invdt = p.invdt; a.dirt = p.dirt; a.M = p.M;
   a.PN = PN; a.U = p.U; a.Z = p.Z; a.ZB = p.ZB; a.XN = p.XN; a.YN = p.YN;
   a.ocx = p.ocx; a.ocy = p.ocy; a.dx = p.dx;
@@ -420,20 +450,22 @@ int proj_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const floa
                     int zlo, int zhi, cudaStream_t st) {
   int rc;
   if ((rc = launch_view_geom(p, d_angs, stride, PN, p.d_vg, p.d_fc, p.d_cvd, st))) return rc;
+  if ((rc = launch_view_order(p.d_vg, PN, p.d_order, p.d_counts, st))) return rc;
   if ((rc = launch_sat_image(p, d_vol, st))) return rc;
-  return launch_fwd(p, p.d_vg, p.d_fc, p.d_cvd, nullptr, PN, d_prj, zlo, zhi, st);
+  return launch_fwd(p, p.d_vg, p.d_fc, p.d_cvd, p.d_order, PN, d_prj, zlo, zhi, st);
 }
 
 int back_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const float* d_prj, float* d_vol,
                     int back_mode, int zlo, int zhi, cudaStream_t st) {
   int rc;
   if ((rc = launch_view_geom(p, d_angs, stride, PN, p.d_vg, p.d_fc, p.d_cvd, st))) return rc;
+  if ((rc = launch_view_order(p.d_vg, PN, p.d_order, p.d_counts, st))) return rc;
   const bool adj = back_mode == DDFAN_BACK_ADJ;
   if ((rc = launch_sat_sino(p, d_prj, PN, adj ? p.d_cvd : nullptr, 1.f, nullptr, nullptr, nullptr, st)))
     return rc;
   BackEpi e{};
   e.out = d_vol; e.mask = p.has_mask ? p.d_mask : nullptr; e.zlo = zlo; e.zhi = zhi;
-  return launch_back(p, back_mode, p.d_vg, p.d_fc, PN, e, st);
+  return launch_back(p, back_mode, p.d_vg, p.d_fc, p.d_order, p.d_counts, PN, e, st);
 }
 
 // Groups of slices sharing one angle list: per-slice angle arrays

@@ -2,7 +2,12 @@
 //
 // Prefix-sum ("SAT") cells.  A table is a 3-D array of cells [line][k][zb]:
 // `line` is the image row/column (or the view, for sinogram tables), k the
-// position along the line, zb a block of 4 consecutive slices.  A cell holds,
+// position along the line, zb a block of 4 consecutive slices.  Within a row
+// (line, k) the z-blocks are grouped in z-tiles of ZL blocks and each tile
+// stores its cells plane by plane (all S_hi of the tile, then all S_lo, then
+// all v), so the ZL lanes that own a tile read each plane as one contiguous
+// ZL*16-byte run: float4 index of plane j of block zb in row r is
+//   (r * ZBp + (zb / ZL) * ZL) * F4 + j * ZL + zb % ZL,  ZBp = ZB rounded up to ZL.  A cell holds,
 // for its 4 slices, the exclusive prefix sum S[k] = sum_{j<k} v[j] and the
 // value v[k] itself, so a linearly interpolated prefix sum at position
 // c in [k, k+1] is S[k] + (c - k) v[k]: one cell per sample.  This is the
@@ -58,9 +63,9 @@ template <> struct Acc4<SAT_FP32> {
     for (int i = 0; i < 4; ++i) r.s[i] = __shfl_up_sync(0xffffffffu, s[i], off);
     return r;
   }
-  __device__ void store(float4* cell, const float (&v)[4]) const {
+  __device__ void store(float4* cell, int ps, const float (&v)[4]) const {
     cell[0] = make_float4(s[0], s[1], s[2], s[3]);
-    cell[1] = make_float4(v[0], v[1], v[2], v[3]);
+    cell[ps] = make_float4(v[0], v[1], v[2], v[3]);
   }
 };
 
@@ -98,7 +103,7 @@ template <> struct Acc4<SAT_HILO> {
     return r;
   }
   // stores the renormalised pair (hi = fl(hi + lo)) so hi differences are clean
-  __device__ void store(float4* cell, const float (&v)[4]) const {
+  __device__ void store(float4* cell, int ps, const float (&v)[4]) const {
     float h[4], l[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -107,8 +112,8 @@ template <> struct Acc4<SAT_HILO> {
       h[i] = s;
     }
     cell[0] = make_float4(h[0], h[1], h[2], h[3]);
-    cell[1] = make_float4(l[0], l[1], l[2], l[3]);
-    cell[2] = make_float4(v[0], v[1], v[2], v[3]);
+    cell[ps] = make_float4(l[0], l[1], l[2], l[3]);
+    cell[2 * ps] = make_float4(v[0], v[1], v[2], v[3]);
   }
 };
 
@@ -129,11 +134,10 @@ template <> struct Acc4<SAT_FP64> {
     for (int i = 0; i < 4; ++i) r.s[i] = __shfl_up_sync(0xffffffffu, s[i], off);
     return r;
   }
-  __device__ void store(float4* cell, const float (&v)[4]) const {
-    double2* d = reinterpret_cast<double2*>(cell);
-    d[0] = make_double2(s[0], s[1]);
-    d[1] = make_double2(s[2], s[3]);
-    cell[2] = make_float4(v[0], v[1], v[2], v[3]);
+  __device__ void store(float4* cell, int ps, const float (&v)[4]) const {
+    *reinterpret_cast<double2*>(cell) = make_double2(s[0], s[1]);
+    *reinterpret_cast<double2*>(cell + ps) = make_double2(s[2], s[3]);
+    cell[2 * ps] = make_float4(v[0], v[1], v[2], v[3]);
   }
 };
 
@@ -145,8 +149,8 @@ template <int M> struct Phi4;
 
 template <> struct Phi4<SAT_FP32> {
   float v[4];
-  __device__ __forceinline__ void load(const float4* cell, float f) {
-    float4 s = __ldg(cell), p = __ldg(cell + 1);
+  __device__ __forceinline__ void load(const float4* cell, int ps, float f) {
+    float4 s = __ldg(cell), p = __ldg(cell + ps);
     v[0] = fmaf(f, p.x, s.x); v[1] = fmaf(f, p.y, s.y);
     v[2] = fmaf(f, p.z, s.z); v[3] = fmaf(f, p.w, s.w);
   }
@@ -160,8 +164,8 @@ template <> struct Phi4<SAT_FP32> {
 
 template <> struct Phi4<SAT_HILO> {
   float hi[4], lo[4];
-  __device__ __forceinline__ void load(const float4* cell, float f) {
-    float4 h = __ldg(cell), l = __ldg(cell + 1), p = __ldg(cell + 2);
+  __device__ __forceinline__ void load(const float4* cell, int ps, float f) {
+    float4 h = __ldg(cell), l = __ldg(cell + ps), p = __ldg(cell + 2 * ps);
     hi[0] = h.x; hi[1] = h.y; hi[2] = h.z; hi[3] = h.w;
     lo[0] = fmaf(f, p.x, l.x); lo[1] = fmaf(f, p.y, l.y);
     lo[2] = fmaf(f, p.z, l.z); lo[3] = fmaf(f, p.w, l.w);
@@ -178,10 +182,10 @@ template <> struct Phi4<SAT_HILO> {
 
 template <> struct Phi4<SAT_FP64> {
   double v[4];
-  __device__ __forceinline__ void load(const float4* cell, float f) {
-    const double2* d = reinterpret_cast<const double2*>(cell);
-    double2 a = __ldg(d), b = __ldg(d + 1);
-    float4 p = __ldg(cell + 2);
+  __device__ __forceinline__ void load(const float4* cell, int ps, float f) {
+    double2 a = __ldg(reinterpret_cast<const double2*>(cell));
+    double2 b = __ldg(reinterpret_cast<const double2*>(cell + ps));
+    float4 p = __ldg(cell + 2 * ps);
     const double fd = (double)f;
     v[0] = fma(fd, (double)p.x, a.x); v[1] = fma(fd, (double)p.y, a.y);
     v[2] = fma(fd, (double)p.z, b.x); v[3] = fma(fd, (double)p.w, b.y);

@@ -100,6 +100,7 @@ struct SatSrc {
   const int* yview;     // line -> view index into y
   const float* rowsum;  // [lines][U] row sums (slice 0) of the subset
   int XN, YN, U, Z;
+  int ZLt;              // z-blocks per z-tile of the output layout
 };
 
 __device__ __forceinline__ void sat_load(const SatSrc& s, int line, int k, int zb,
@@ -120,6 +121,10 @@ __device__ __forceinline__ void sat_load(const SatSrc& s, int line, int k, int z
     m = s.wgt ? __ldg(s.wgt + e) * s.wscale : s.wscale;
   }
   const int z0 = zb * 4;
+  if (z0 >= s.Z) {  // padding block of the last z-tile
+    v[0] = v[1] = v[2] = v[3] = 0.f;
+    return;
+  }
   if ((s.Z & 3) == 0) {
     const float4 q = __ldg(reinterpret_cast<const float4*>(s.a + base + z0));
     v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
@@ -193,292 +198,19 @@ __global__ void __launch_bounds__(256) k_sat(SatSrc s, float4* __restrict__ out,
   for (int j = 0; j < C; ++j) {
     const int k = k0 + j;
     if (k < Nw) {
-      run.store(out + (((size_t)line * Nw + k) * ZB + zb) * F4, v[j]);
+      const int zt = zb / s.ZLt;
+      run.store(out + (((size_t)line * Nw + k) * ZB + (size_t)zt * s.ZLt) * F4 + (zb - zt * s.ZLt), s.ZLt,
+                v[j]);
       run.add(v[j]);
     }
   }
 }
 
-// ============================================================ forward projector
+}  // namespace ddfan
 
-struct FwdArgs {
-  const float4* satx;  // image rows table  [YN][XN][ZB]
-  const float4* saty;  // image columns table [XN][YN][ZB]
-  const ViewGeom* vg;
-  const double2* fc;   // [PN][U+1]
-  const float* cvd;    // [PN][U]
-  const int* order;    // CTA row -> view (null = identity)
-  float* out;          // [PN][U][Z]
-  int PN, U, Z, ZB, XN, YN;
-  float dx;
-  int zlo, zhi;
-};
+#include "ddfan_proj_kernels.cuh"
 
-// Branchless DD forward projection (AAPM_script/MultiSlicesProjGPU.cu:100-200)
-// with exact interpolation weights.  Thread = CG consecutive channels x 4
-// slices of one view; for every line ii it samples the U+1 shared boundary
-// rays once each (channel u uses boundaries u and u+1) and adds
-// (Phi(c_{u+1}) - Phi(c_u)) / len_u, len_u the footprint length in mm.
-template <int M, int ZL, int CG>
-__global__ void __launch_bounds__(128) k_fwd(FwdArgs a) {
-  constexpr int F4 = CellInfo<M>::F4;
-  constexpr int NG = 32 / ZL;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int zl = lane % ZL, g = lane / ZL;
-  const int p = a.order ? a.order[blockIdx.y] : blockIdx.y;
-  const int zb = blockIdx.z * ZL + zl;
-  const int u0 = ((blockIdx.x * 4 + w) * NG + g) * CG;
-  if (u0 >= a.U || zb >= a.ZB) return;  // no block-level synchronisation below
-  const bool xm = a.vg[p].xmajor != 0;
-  const int nl = xm ? a.XN : a.YN, N = xm ? a.YN : a.XN;
-  const float4* sat = xm ? a.saty : a.satx;
-  const size_t rowstride = (size_t)a.ZB * F4;  // one k step
-  double F[CG + 1], Cc[CG + 1];
-#pragma unroll
-  for (int b = 0; b <= CG; ++b) {
-    const int ub = min(u0 + b, a.U);
-    const double2 t = a.fc[(size_t)p * (a.U + 1) + ub];
-    F[b] = t.x;
-    Cc[b] = t.y;
-  }
-  float acc[CG][4];
-#pragma unroll
-  for (int b = 0; b < CG; ++b) acc[b][0] = acc[b][1] = acc[b][2] = acc[b][3] = 0.f;
-  const double Nd = (double)N;
-  const float4* base = sat + (size_t)zb * F4;
-  for (int ii = 0; ii < nl; ++ii) {
-    const float4* line = base + (size_t)ii * N * rowstride;
-    const double di = (double)ii;
-    Phi4<M> prev;
-    double cprev = 0.0;
-#pragma unroll
-    for (int b = 0; b <= CG; ++b) {
-      const double c = fma(di, F[b], Cc[b]);
-      const double cc = fmin(fmax(c, 0.0), Nd);
-      const int i0 = min((int)cc, N - 1);
-      const float f = (float)(cc - (double)i0);
-      Phi4<M> ph;
-      ph.load(line + (size_t)i0 * rowstride, f);
-      if (b > 0) {
-        const float inv = __frcp_rn((float)(c - cprev) * a.dx);
-        float d[4];
-        ph.diff(prev, d);
-#pragma unroll
-        for (int s = 0; s < 4; ++s) acc[b - 1][s] = fmaf(d[s], inv, acc[b - 1][s]);
-      }
-      prev = ph;
-      cprev = c;
-    }
-  }
-#pragma unroll
-  for (int b = 0; b < CG; ++b) {
-    const int u = u0 + b;
-    if (u >= a.U) break;
-    const float cv = __ldg(a.cvd + (size_t)p * a.U + u) * a.dx;
-    float* o = a.out + ((size_t)p * a.U + u) * a.Z;
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-      const int z = zb * 4 + s;
-      if (z >= a.zlo && z < a.zhi) o[z] = acc[b][s] * cv;
-    }
-  }
-}
-
-// ============================================================ backprojectors
-
-struct BackEpi {
-  float* out;            // [YN][XN][Z]
-  const float* addend;   // added before the update (null = none)
-  const float* xin;      // OS-SART: x_new = x_in + t / colSum (null = plain backprojection)
-  const float* colsum;   // [YN][XN] column sums (slice 0), used with xin
-  int nonneg;            // clamp the updated image at 0
-  const uint8_t* mask;   // [YN][XN] or null
-  int zlo, zhi;
-};
-
-__device__ __forceinline__ void back_store(const BackEpi& e, int ix, int iy, int zb, int XN, int Z,
-                                           bool scale_by_mask, const float (&acc)[4]) {
-  const size_t pix = (size_t)iy * XN + ix;
-  const float m = e.mask ? (float)e.mask[pix] : 1.f;
-  const float cs = e.xin ? __ldg(e.colsum + pix) : 0.f;
-#pragma unroll
-  for (int s = 0; s < 4; ++s) {
-    const int z = zb * 4 + s;
-    if (z < e.zlo || z >= e.zhi) continue;
-    const size_t idx = pix * Z + z;
-    float val = scale_by_mask ? acc[s] * m : (m != 0.f ? acc[s] : 0.f);
-    if (e.addend) val += e.addend[idx];
-    if (e.xin) {
-      // x += t / colSum where colSum != 0, else x += t (AAPM_script/OSSART_AAPM.m:94-97)
-      const float t = cs != 0.f ? __fdiv_rn(val, cs) : val;
-      val = e.xin[idx] + t;
-      if (e.nonneg) val = fmaxf(val, 0.f);
-    }
-    e.out[idx] = val;
-  }
-}
-
-struct RefArgs {
-  const float4* satq;   // sinogram table [PN][U+1][ZB]
-  const ViewGeom* vg;
-  int PN, U, Z, ZB, XN, YN;
-  double ocx, ocy, dx, inv_sid, inv_dbeta, cnt;  // cnt = detCntIdx + 1 - 0.5
-  BackEpi epi;
-};
-
-// Reference backprojector formula (AAPM_script/MultiSlicesBackGPU.cu:115-184):
-// voxel-driven, angular detector coordinate alpha = asin(cross / (|s| l)),
-// footprint half-width dx * ddv / (2 l^2), weight dx l / ddv, coordinate
-// alpha / dbeta + detCntIdx + 1 -- all evaluated in double, then the two
-// samples of the channel prefix-sum table are differenced in table precision.
-// Thread = VG consecutive voxels along x of one row x 4 slices.
-template <int M, int ZL, int VG>
-__global__ void __launch_bounds__(128) k_back_ref(RefArgs a) {
-  constexpr int F4 = CellInfo<M>::F4;
-  constexpr int NG = 32 / ZL;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int zl = lane % ZL, g = lane / ZL;
-  const int zb = blockIdx.z * ZL + zl;
-  const int nseg = (a.XN + VG - 1) / VG;
-  const int seg = (blockIdx.x * 4 + w) * NG + g;
-  if (seg >= nseg * a.YN || zb >= a.ZB) return;
-  const int iy = seg / nseg, ix0 = (seg % nseg) * VG;
-  const int nv = min(VG, a.XN - ix0);
-  unsigned on = 0;
-#pragma unroll
-  for (int v = 0; v < VG; ++v)
-    if (v < nv && (!a.epi.mask || a.epi.mask[(size_t)iy * a.XN + ix0 + v] != 0)) on |= 1u << v;
-  float acc[VG][4];
-#pragma unroll
-  for (int v = 0; v < VG; ++v) acc[v][0] = acc[v][1] = acc[v][2] = acc[v][3] = 0.f;
-  const double vy = (iy - a.ocy) * a.dx;
-  const double Ud = (double)a.U;
-  const size_t rowstride = (size_t)a.ZB * F4;
-  for (int p = 0; p < a.PN; ++p) {
-    const double sx = a.vg[p].sx, sy = a.vg[p].sy;
-    const bool selx = fabs(sx) > fabs(sy);
-    const float4* base = a.satq + ((size_t)p * (a.U + 1) * a.ZB + zb) * F4;
-#pragma unroll
-    for (int v = 0; v < VG; ++v) {
-      if (!(on >> v & 1u)) continue;
-      const double vx = (ix0 + v - a.ocx) * a.dx;
-      const double ddx = vx - sx, ddy = vy - sy;
-      const double l2 = ddx * ddx + ddy * ddy;
-      const double l = sqrt(l2);
-      const double alpha = asin((sy * ddx - sx * ddy) * a.inv_sid / l);
-      const double ddv = selx ? ddx : ddy;
-      const double da = ddv / l2 * a.dx * 0.5;
-      const float cosv = (float)(a.dx / ddv * l);
-      const double cL = fmin(fmax((alpha - da) * a.inv_dbeta + a.cnt, 0.0), Ud);
-      const double cR = fmin(fmax((alpha + da) * a.inv_dbeta + a.cnt, 0.0), Ud);
-      const int iL = min((int)cL, a.U - 1), iR = min((int)cR, a.U - 1);
-      Phi4<M> pL, pR;
-      pL.load(base + (size_t)iL * rowstride, (float)(cL - iL));
-      pR.load(base + (size_t)iR * rowstride, (float)(cR - iR));
-      float d[4];
-      pR.diff(pL, d);
-#pragma unroll
-      for (int s = 0; s < 4; ++s) acc[v][s] = fmaf(d[s], cosv, acc[v][s]);
-    }
-  }
-#pragma unroll
-  for (int v = 0; v < VG; ++v)
-    if (v < nv) back_store(a.epi, ix0 + v, iy, zb, a.XN, a.Z, false, acc[v]);
-}
-
-struct AdjArgs {
-  const float4* satq;   // weighted sinogram table [PN][U+1][ZB], weight r_u / |dir_u.axis|
-  const ViewGeom* vg;
-  const double2* fc;    // [PN][U+1]
-  const float* tb;      // fan tangents of the boundaries, increasing, U+1
-  const uint16_t* lut;  // bracket lookup, M entries
-  float t0, invdt, dirt;
-  int M;
-  int PN, U, Z, ZB, XN, YN;
-  double ocx, ocy, dx;
-  BackEpi epi;
-};
-
-// Exact transpose of k_fwd.  For a view integrated along lines ii, pixel k of
-// line ii receives sum_u w_u * (fraction of footprint u inside [k, k+1]),
-// w_u = r_u / |dir_u.axis| -- which is the difference of the channel prefix
-// sum Q of w at the fractional boundary index beta of the pixel's two edges:
-// beta(c) = b + (c - c_b(ii)) / (c_{b+1}(ii) - c_b(ii)) with the forward's own
-// c_b(ii).  Thread = VG consecutive pixels along one line (so VG+1 edges)
-// x 4 slices; XM selects the lines (x columns for xmajor views, y rows
-// otherwise) and the kernel visits only the views of that orientation.
-template <int M, int ZL, int VG, bool XM>
-__global__ void __launch_bounds__(128) k_back_adj(AdjArgs a) {
-  constexpr int F4 = CellInfo<M>::F4;
-  constexpr int NG = 32 / ZL;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int zl = lane % ZL, g = lane / ZL;
-  const int zb = blockIdx.z * ZL + zl;
-  const int nl = XM ? a.XN : a.YN, N = XM ? a.YN : a.XN;
-  const int nseg = (N + VG - 1) / VG;
-  const int seg = (blockIdx.x * 4 + w) * NG + g;
-  if (seg >= nseg * nl || zb >= a.ZB) return;
-  const int ii = seg / nseg, k0 = (seg % nseg) * VG;
-  const int nv = min(VG, N - k0);
-  float acc[VG][4];
-#pragma unroll
-  for (int v = 0; v < VG; ++v) acc[v][0] = acc[v][1] = acc[v][2] = acc[v][3] = 0.f;
-  const double lineX = (ii - (XM ? a.ocx : a.ocy)) * a.dx;  // world coordinate of the line
-  const double ock = XM ? a.ocy : a.ocx;
-  const double di = (double)ii;
-  const size_t rowstride = (size_t)a.ZB * F4;
-  const float tfirst = __ldg(a.tb), tlast = __ldg(a.tb + a.U);
-  for (int p = 0; p < a.PN; ++p) {
-    if ((a.vg[p].xmajor != 0) != XM) continue;
-    const double sx = a.vg[p].sx, sy = a.vg[p].sy;
-    const float shx = a.vg[p].shx, shy = a.vg[p].shy, sgn = a.vg[p].sgn;
-    const float4* base = a.satq + ((size_t)p * (a.U + 1) * a.ZB + zb) * F4;
-    const double2* fcp = a.fc + (size_t)p * (a.U + 1);
-    Phi4<M> prev;
-#pragma unroll
-    for (int e = 0; e <= VG; ++e) {
-      if (e > nv) break;
-      const double ck = (double)(k0 + e);             // edge position (texel-sample coords)
-      const double along = (ck - 0.5 - ock) * a.dx;   // its world coordinate along the line
-      const float vx = (float)((XM ? lineX : along) - sx);
-      const float vy = (float)((XM ? along : lineX) - sy);
-      const float cr = shx * vy - shy * vx, dt = shx * vx + shy * vy;
-      const float t = a.dirt * __fdividef(cr, dt);
-      int b;
-      float frac = 0.f;
-      if (!(t >= tfirst)) {
-        b = 0;
-      } else if (t >= tlast) {
-        b = a.U;
-      } else {
-        const int m = (int)fminf(fmaxf((t - a.t0) * a.invdt, 0.f), (float)(a.M - 1));
-        b = __ldg(a.lut + m);
-        int guard = 0;
-        while (b < a.U - 1 && __ldg(a.tb + b + 1) <= t && guard++ < 64) ++b;
-        while (b > 0 && __ldg(a.tb + b) > t && guard++ < 128) --b;
-        const double2 f0 = __ldg(fcp + b), f1 = __ldg(fcp + b + 1);
-        const double c0 = fma(di, f0.x, f0.y), c1 = fma(di, f1.x, f1.y);
-        frac = __fdiv_rn((float)(ck - c0), (float)(c1 - c0));
-        frac = fminf(fmaxf(frac, 0.f), 1.f);
-      }
-      Phi4<M> ph;
-      ph.load(base + (size_t)b * rowstride, frac);
-      if (e > 0) {
-        float d[4];
-        ph.diff(prev, d);
-#pragma unroll
-        for (int s = 0; s < 4; ++s) acc[e - 1][s] = fmaf(sgn, d[s], acc[e - 1][s]);
-      }
-      prev = ph;
-    }
-  }
-#pragma unroll
-  for (int v = 0; v < VG; ++v) {
-    if (v >= nv) break;
-    const int k = k0 + v;
-    back_store(a.epi, XM ? ii : k, XM ? k : ii, zb, a.XN, a.Z, true, acc[v]);
-  }
-}
+namespace ddfan {
 
 // ============================================================ OS-SART helpers
 

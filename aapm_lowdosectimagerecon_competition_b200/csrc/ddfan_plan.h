@@ -51,6 +51,8 @@ struct Plan {
   float* d_cvd = nullptr;
   float* d_tmp = nullptr;   // one image of scratch (exact adjoint, pass 1)
   float* d_angs = nullptr;  // PNmax angles (host-angle entry points)
+  int* d_order = nullptr;   // PNmax views in dispatch order (x-major first)
+  int* d_counts = nullptr;  // {x-major views, others}
   size_t bytes = 0;
 };
 
@@ -64,8 +66,9 @@ int launch_sat_sino(const Plan& p, const float* d_prj, int PN, const float* wgt,
                     const float* y, const int* yview, const float* rowsum, cudaStream_t st);
 int launch_fwd(const Plan& p, const ViewGeom* vg, const double2* fc, const float* cvd,
                const int* order, int PN, float* d_prj, int zlo, int zhi, cudaStream_t st);
-int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2* fc, int PN,
-                const BackEpi& epi, cudaStream_t st);
+int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2* fc,
+                const int* order, const int* counts, int PN, const BackEpi& epi, cudaStream_t st);
+int launch_view_order(const ViewGeom* vg, int PN, int* order, int* counts, cudaStream_t st);
 int proj_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const float* d_vol,
                     float* d_prj, int zlo, int zhi, cudaStream_t st);
 int back_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const float* d_prj,

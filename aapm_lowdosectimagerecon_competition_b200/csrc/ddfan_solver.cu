@@ -174,7 +174,8 @@ struct Solver {
   double2* d_fc = nullptr;
   float* d_cvd = nullptr;
   int* d_yview = nullptr;  // subset-ordered row -> original view index
-  int* d_order = nullptr;  // per subset: forward CTA order (x-major views first)
+  int* d_order = nullptr;  // per subset: views in dispatch order (x-major first)
+  int* d_counts = nullptr; // per subset: {x-major views, others}
   float* d_rows = nullptr; // [PNall][U]   row sums, subset order
   float* d_cols = nullptr; // [nsub][YN][XN] column sums
   float* d_y = nullptr;    // [PNall][U][Z] measured sinogram, original order
@@ -197,7 +198,7 @@ static void solver_free(Solver* s) {
   if (s->gexec) cudaGraphExecDestroy(s->gexec);
   if (s->graph) cudaGraphDestroy(s->graph);
   if (s->own) cudaStreamDestroy(s->own);
-  void* ptrs[] = {s->d_vg, s->d_fc, s->d_cvd, s->d_yview, s->d_order, s->d_rows, s->d_cols,
+  void* ptrs[] = {s->d_vg, s->d_fc, s->d_cvd, s->d_yview, s->d_order, s->d_counts, s->d_rows, s->d_cols,
                   s->d_y, s->d_x, s->d_xprev, s->d_ax, s->d_t};
   for (void* q : ptrs)
     if (q) cudaFree(q);
@@ -239,7 +240,7 @@ static int solver_iteration(Solver& s, cudaStream_t st) {
     BackEpi e{};
     e.out = s.d_x; e.xin = s.d_x; e.colsum = s.d_cols + (size_t)k * s.XN * s.YN;
     e.nonneg = s.nonneg; e.mask = p.has_mask ? p.d_mask : nullptr; e.zlo = 0; e.zhi = s.Z;
-    if ((rc = launch_back(p, s.back_mode, vg, fc, c, e, st))) return rc;
+    if ((rc = launch_back(p, s.back_mode, vg, fc, s.d_order + o, s.d_counts + 2 * k, c, e, st))) return rc;
     n += adj ? 5 : 4;
   }
   if (s.useFISTA) {
@@ -297,7 +298,7 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
   const size_t V = (size_t)XN * YN * SLN;
   if ((rc = salloc(s, &s.d_vg, PNall)) || (rc = salloc(s, &s.d_fc, (size_t)PNall * (DNU + 1))) ||
       (rc = salloc(s, &s.d_cvd, (size_t)PNall * DNU)) || (rc = salloc(s, &s.d_yview, PNall)) ||
-      (rc = salloc(s, &s.d_order, PNall)) || (rc = salloc(s, &s.d_rows, (size_t)PNall * DNU)) ||
+      (rc = salloc(s, &s.d_order, PNall)) || (rc = salloc(s, &s.d_counts, 2 * (size_t)numOfOS)) || (rc = salloc(s, &s.d_rows, (size_t)PNall * DNU)) ||
       (rc = salloc(s, &s.d_cols, (size_t)numOfOS * XN * YN)) ||
       (rc = salloc(s, &s.d_y, (size_t)PNall * DNU * SLN)) || (rc = salloc(s, &s.d_x, V)) ||
       (rc = salloc(s, &s.d_xprev, V)) || (rc = salloc(s, &s.d_ax, (size_t)PNmax * DNU * SLN)) ||
@@ -311,19 +312,11 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
   DDFAN_CK(cudaMemcpyAsync(dang.p, angs.data(), sizeof(float) * PNall, cudaMemcpyHostToDevice, st));
   DDFAN_CK(cudaMemcpyAsync(s.d_yview, yview.data(), sizeof(int) * PNall, cudaMemcpyHostToDevice, st));
   if ((rc = launch_view_geom(*s.P, dang.p, 1, PNall, s.d_vg, s.d_fc, s.d_cvd, st))) return rc;
-  // forward CTA order per subset: views of one orientation together (one
-  // image table at a time stays hot in L2)
-  std::vector<ViewGeom> hvg(PNall);
-  DDFAN_CK(cudaMemcpyAsync(hvg.data(), s.d_vg, sizeof(ViewGeom) * PNall, cudaMemcpyDeviceToHost, st));
-  DDFAN_CK(cudaStreamSynchronize(st));
-  std::vector<int> order(PNall);
-  for (int k = 0; k < numOfOS; ++k) {
-    int w = s.off[k];
-    for (int pass = 1; pass >= 0; --pass)
-      for (int i = 0; i < s.cnt[k]; ++i)
-        if (hvg[s.off[k] + i].xmajor == pass) order[w++] = i;
-  }
-  DDFAN_CK(cudaMemcpyAsync(s.d_order, order.data(), sizeof(int) * PNall, cudaMemcpyHostToDevice, st));
+  // per subset: views of one orientation together (one image table at a
+  // time stays hot in L2; the exact adjoint visits each orientation in turn)
+  for (int k = 0; k < numOfOS; ++k)
+    if ((rc = launch_view_order(s.d_vg + s.off[k], s.cnt[k], s.d_order + s.off[k], s.d_counts + 2 * k, st)))
+      return rc;
   // row / column sums from slice 0 on a one-slice plan (AAPM_script/OSSART_AAPM.m:59-66)
   {
     PlanDesc d1 = d;
@@ -339,7 +332,7 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
     for (int k = 0; k < numOfOS; ++k) {
       const int o = s.off[k], c = s.cnt[k];
       if ((rc = launch_fwd(*P1.p, s.d_vg + o, s.d_fc + (size_t)o * (DNU + 1), s.d_cvd + (size_t)o * DNU,
-                           nullptr, c, s.d_rows + (size_t)o * DNU, 0, 1, st)))
+                           s.d_order + o, c, s.d_rows + (size_t)o * DNU, 0, 1, st)))
         return rc;
     }
     for (int k = 0; k < numOfOS; ++k) {
@@ -352,7 +345,8 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
       e.out = s.d_cols + (size_t)k * XN * YN;
       e.mask = P1.p->has_mask ? P1.p->d_mask : nullptr;
       e.zlo = 0; e.zhi = 1;
-      if ((rc = launch_back(*P1.p, back_mode, s.d_vg + o, s.d_fc + (size_t)o * (DNU + 1), c, e, st)))
+      if ((rc = launch_back(*P1.p, back_mode, s.d_vg + o, s.d_fc + (size_t)o * (DNU + 1), s.d_order + o,
+                            s.d_counts + 2 * k, c, e, st)))
         return rc;
     }
     DDFAN_CK(cudaStreamSynchronize(st));

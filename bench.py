@@ -45,7 +45,46 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--kernels", action="store_true",
+                    help="time only one subset's projector kernels (small case for ncu captures)")
     return ap.parse_args()
+
+
+def run_kernels(args):
+    """One 96-view subset of the workload through the device Plan API:
+    forward, exact-adjoint and reference backprojection, `steps` times each
+    after `warmup` rounds.  Prints per-call device ms (CUDA events)."""
+    import torch
+    from aapm_lowdosectimagerecon_competition_b200 import dd2, device
+    dev = torch.device("cuda", 0)
+    s = workload(args.slices)
+    x0, y0, xds, yds = dd2.fan_geometry(s.sid, s.sdd, s.DNU, s.detCellWidth, s.detCntIdx)
+    angs = torch.from_numpy(np.ascontiguousarray(s.angles()[::s.numOfOS])).to(dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(1)
+    vol = torch.rand((s.YN, s.XN, s.SLN), device=dev, generator=g) * 0.02
+    pl = device.Plan(x0, y0, s.DNU, xds, yds, s.detCntIdx, s.XN, s.YN, s.SLN, angs.numel(), s.dx,
+                     sat=args.sat)
+    prj = pl.proj(angs, vol)
+    out = torch.empty_like(vol)
+    calls = {"proj": lambda: pl.proj(angs, vol, out=prj),
+             "back_adj": lambda: pl.back(angs, prj, out=out, mode="adj"),
+             "back_ref": lambda: pl.back(angs, prj, out=out, mode="ref")}
+    res = {}
+    for name, fn in calls.items():
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        res[name + "_ms"] = e0.elapsed_time(e1) / max(args.steps, 1)
+    pl.close()
+    print(json.dumps({"kernels": res, "sat": args.sat, "views": int(angs.numel()),
+                      "image": [s.XN, s.YN, s.SLN]}), flush=True)
 
 
 def workload(slices):
@@ -372,6 +411,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.kernels:
+        run_kernels(args)
     else:
         run_ours(args)
 
