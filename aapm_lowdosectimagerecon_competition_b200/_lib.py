@@ -34,6 +34,7 @@ SIGNATURES = {
     "ddfan_plan_device_bytes": (_sz, [_p]),
     "ddfan_proj_dev": (_i, [_p, _p, _i, _i, _p, _p, _p]),
     "ddfan_back_dev": (_i, [_p, _p, _i, _i, _p, _p, _i, _p]),
+    "ddfan_proj_noalloc": (_i, [_f, _f, _i, _p, _p, _f, _f, _p, _i, _i, _i, _i, _p, _f, _p, _i, _p, _p]),
     "ddfan_ossart_create": (_i, [_p, _f, _f, _i, _p, _p, _f, _f, _f, _p, _i, _i, _i, _i, _f, _p, _i,
                                  _i, _i, _i, _i, _i]),
     "ddfan_ossart_destroy": (None, [_p]),

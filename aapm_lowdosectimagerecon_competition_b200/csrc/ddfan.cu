@@ -68,7 +68,7 @@ LaunchProfiler::~LaunchProfiler() {
 // but a stack of ZB blocks is padded to whole tiles.  Relative cost per
 // padded block of each width (measured on the 512^2 x 128 workload: widths
 // 8, 4, 2 ran at 1 : 1.2 : 2.1); pick the cheapest padded stack.
-static int pow2_zl(int ZB) {
+int pow2_zl(int ZB) {
   const int widths[4] = {8, 4, 2, 1};
   const double cost[4] = {1.0, 1.2, 2.1, 3.6};
   int best = 1;
@@ -112,7 +112,7 @@ void plan_free(Plan* P) {
 
 // DD3Boundaries (AAPM_script/utilities.cuh:268-287): evaluated in double,
 // stored as float like the reference's float arrays.
-static void boundaries(int n, const float* c, std::vector<double>& out) {
+void boundaries(int n, const float* c, std::vector<double>& out) {
   const int nb = n + 1;
   out.assign(nb, 0.0);
   if (nb >= 3) {

@@ -1,0 +1,140 @@
+// ddfan_noalloc.cu -- forward projection that allocates no device memory.
+//
+// ddfan_proj_dev needs a plan, and a plan holds cudaMalloc'd prefix-sum and
+// geometry tables.  Some callers cannot allocate: their device memory is
+// owned up front by another allocator (a framework's caching allocator or a
+// pool reserved at start-up), or they cannot afford cudaMalloc's implicit
+// device-wide synchronisation in the middle of a pipeline.  For them,
+// ddfan_proj_noalloc runs the same kernels with every scratch table placed
+// in one file-scope device array of DDFAN_NOALLOC_SCRATCH_BYTES.  The array
+// exists on every GPU that loads this library, for as long as it stays
+// loaded.  Calls share it, so two calls whose kernels overlap on a GPU race
+// on it: issue them on one stream, or order them.
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "ddfan.h"
+#include "ddfan_kernels.cuh"
+#include "ddfan_plan.h"
+
+namespace ddfan {
+namespace {
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[DDFAN_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_addr_mutex;
+void* g_addr[kMaxDevices] = {};
+
+// Device address of the scratch array on `dev` (the current device).  In host
+// code the array's name only stands in for it, so the address is looked up
+// once per device with cudaGetSymbolAddress.
+int scratch_address(int dev, unsigned char** out) {
+  if (dev < 0 || dev >= kMaxDevices) return set_err(DDFAN_ERR_UNSUPPORTED, "device index %d", dev);
+  std::lock_guard<std::mutex> lock(g_addr_mutex);
+  if (!g_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      return set_err(DDFAN_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+    }
+    g_addr[dev] = p;
+  }
+  *out = static_cast<unsigned char*>(g_addr[dev]);
+  return DDFAN_OK;
+}
+
+size_t align256(size_t n) { return (n + 255) / 256 * 256; }
+
+}  // namespace
+}  // namespace ddfan
+
+using namespace ddfan;
+
+extern "C" DDFAN_API int ddfan_proj_noalloc(float x0, float y0, int DNU, const float* xds,
+                                            const float* yds, float imgXCenter, float imgYCenter,
+                                            const float* d_angs, int PN, int XN, int YN, int SLN,
+                                            const float* d_vol, float dx, const uint8_t* mask,
+                                            int sat_mode, float* d_prj, void* stream) {
+  if (!xds || !yds || !d_angs || !d_vol || !d_prj) return set_err(DDFAN_ERR_ARG, "proj_noalloc: null argument");
+  if (DNU < 2 || DNU + 1 > 1024 || XN < 1 || YN < 1 || XN > 1024 || YN > 1024 || SLN < 1 || PN < 1 ||
+      PN > 65535)
+    return set_err(DDFAN_ERR_ARG, "proj_noalloc: bad sizes (DNU=%d XN=%d YN=%d SLN=%d PN=%d)", DNU, XN, YN,
+                   SLN, PN);
+  if (!(dx > 0.f)) return set_err(DDFAN_ERR_ARG, "proj_noalloc: dx must be > 0");
+  if (sat_mode < SAT_FP32 || sat_mode > SAT_FP64) return set_err(DDFAN_ERR_ARG, "proj_noalloc: sat_mode %d", sat_mode);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(DDFAN_ERR_CUDA, "proj_noalloc: no current CUDA device");
+  }
+  // a plan on the host stack whose device tables all point into the scratch array
+  Plan p;
+  p.device = dev;
+  p.XN = XN; p.YN = YN; p.U = DNU; p.Z = SLN; p.ZB = (SLN + 3) / 4;
+  p.PNmax = PN; p.mode = sat_mode; p.ZL = pow2_zl(p.ZB);
+  p.ZB = (p.ZB + p.ZL - 1) / p.ZL * p.ZL;
+  p.x0 = x0; p.y0 = y0; p.dx = dx;
+  p.ocx = (XN - 1.0) * 0.5 - (double)imgXCenter / (double)dx;
+  p.ocy = (YN - 1.0) * 0.5 - (double)imgYCenter / (double)dx;
+  boundaries(DNU, xds, p.bx);
+  boundaries(DNU, yds, p.by);
+  std::vector<double> xd(xds, xds + DNU), yd(yds, yds + DNU);
+  p.has_mask = mask != nullptr;
+  // carve the scratch array (every region is fully rewritten by each call:
+  // nothing needs to start at zero)
+  const size_t cells = (size_t)XN * YN * p.ZB * cell_f4(sat_mode);
+  size_t off = 0;
+  auto take = [&](size_t bytes) { const size_t o = off; off += align256(bytes); return o; };
+  const size_t o_bx = take(sizeof(double) * (DNU + 1)), o_by = take(sizeof(double) * (DNU + 1));
+  const size_t o_xd = take(sizeof(double) * DNU), o_yd = take(sizeof(double) * DNU);
+  const size_t o_mask = take(mask ? (size_t)XN * YN : 0);
+  const size_t o_vg = take(sizeof(ViewGeom) * PN), o_fc = take(sizeof(double2) * PN * (DNU + 1));
+  const size_t o_cvd = take(sizeof(float) * PN * DNU), o_ord = take(sizeof(int) * PN);
+  const size_t o_cnt = take(sizeof(int) * 2);
+  const size_t o_satx = take(sizeof(float4) * cells), o_saty = take(sizeof(float4) * cells);
+  if (off > DDFAN_NOALLOC_SCRATCH_BYTES)
+    return set_err(DDFAN_ERR_UNSUPPORTED,
+                   "proj_noalloc: this problem needs %zu bytes of scratch, the fixed scratch array holds %llu "
+                   "(use ddfan_plan_create + ddfan_proj_dev)",
+                   off, (unsigned long long)DDFAN_NOALLOC_SCRATCH_BYTES);
+  unsigned char* base = nullptr;
+  int rc = scratch_address(dev, &base);
+  if (rc) return rc;
+  p.d_bx = reinterpret_cast<double*>(base + o_bx);
+  p.d_by = reinterpret_cast<double*>(base + o_by);
+  p.d_xd = reinterpret_cast<double*>(base + o_xd);
+  p.d_yd = reinterpret_cast<double*>(base + o_yd);
+  p.d_mask = mask ? base + o_mask : nullptr;
+  p.d_vg = reinterpret_cast<ViewGeom*>(base + o_vg);
+  p.d_fc = reinterpret_cast<double2*>(base + o_fc);
+  p.d_cvd = reinterpret_cast<float*>(base + o_cvd);
+  p.d_order = reinterpret_cast<int*>(base + o_ord);
+  p.d_counts = reinterpret_cast<int*>(base + o_cnt);
+  p.d_satx = reinterpret_cast<float4*>(base + o_satx);
+  p.d_saty = reinterpret_cast<float4*>(base + o_saty);
+  cudaStream_t st = (cudaStream_t)stream;
+  // host -> scratch copies of the small geometry arrays (pageable sources are
+  // staged before cudaMemcpyAsync returns)
+  cudaError_t e = cudaMemcpyAsync(p.d_bx, p.bx.data(), sizeof(double) * (DNU + 1), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(p.d_by, p.by.data(), sizeof(double) * (DNU + 1), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(p.d_xd, xd.data(), sizeof(double) * DNU, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(p.d_yd, yd.data(), sizeof(double) * DNU, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && mask) e = cudaMemcpyAsync(p.d_mask, mask, (size_t)XN * YN, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(DDFAN_ERR_CUDA, "proj_noalloc: geometry upload: %s", cudaGetErrorString(e));
+  }
+  if ((rc = launch_view_geom(p, d_angs, 1, PN, p.d_vg, p.d_fc, p.d_cvd, st))) return rc;
+  if ((rc = launch_view_order(p.d_vg, PN, p.d_order, p.d_counts, st))) return rc;
+  if ((rc = launch_sat_image(p, d_vol, st))) return rc;
+  rc = launch_fwd(p, p.d_vg, p.d_fc, p.d_cvd, p.d_order, PN, d_prj, 0, SLN, st);
+  // the stack plan does not own its device pointers
+  p.d_bx = p.d_by = p.d_xd = p.d_yd = nullptr;
+  return rc;
+}

@@ -57,6 +57,10 @@ struct Plan {
 };
 
 int plan_create(Plan** out, const PlanDesc& d);
+// z-blocks per z-tile for a stack of ZB 4-slice blocks
+int pow2_zl(int ZB);
+// DD3Boundaries (AAPM_script/utilities.cuh:268-287), float-rounded like the reference stores them
+void boundaries(int n, const float* c, std::vector<double>& out);
 void plan_free(Plan* p);
 
 int launch_view_geom(const Plan& p, const float* d_angs, int stride, int PN, ViewGeom* vg,

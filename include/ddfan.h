@@ -113,6 +113,27 @@ DDFAN_API int ddfan_proj_dev(ddfan_plan* plan, const float* d_angs, int PN, int 
 DDFAN_API int ddfan_back_dev(ddfan_plan* plan, const float* d_angs, int PN, int angs_per_slice,
                              const float* d_prj, float* d_vol, int back_mode, void* stream);
 
+/* Forward projection that allocates no device memory.  No counterpart in the
+ * reference.  For callers that cannot call cudaMalloc: their device memory is
+ * owned up front by another allocator (a framework's caching allocator, a pool
+ * reserved at start-up), or they cannot take cudaMalloc's implicit device-wide
+ * synchronisation mid-pipeline.  Same result as ddfan_proj_dev on a plan of the
+ * same geometry; device inputs d_angs[PN] (one angle list for all slices) and
+ * d_vol[YN][XN][SLN], device output d_prj[PN][DNU][SLN]; xds, yds and mask
+ * (may be NULL) are host arrays.  Runs on the calling thread's current device.
+ * All scratch (geometry and prefix-sum tables) lives in one fixed device array
+ * of DDFAN_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds
+ * until exit; a problem needing more returns DDFAN_ERR_UNSUPPORTED before any
+ * GPU work.  The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress): make it before capturing a stream.  Calls share the
+ * array, so calls whose kernels overlap on one GPU race: serialise them (one
+ * stream, or events). */
+#define DDFAN_NOALLOC_SCRATCH_BYTES (64ull << 20)
+DDFAN_API int ddfan_proj_noalloc(float x0, float y0, int DNU, const float* xds, const float* yds,
+                                 float imgXCenter, float imgYCenter, const float* d_angs, int PN,
+                                 int XN, int YN, int SLN, const float* d_vol, float dx,
+                                 const uint8_t* mask, int sat_mode, float* d_prj, void* stream);
+
 /* ---- OS-SART / FISTA solver with device-resident state ----
  * Replaces AAPM_script/OSSART_AAPM.m:33-118.  Subset k holds views
  * k, k + numOfOS, ... (:60); row/column sums come from slice 0 (:61-64);
