@@ -24,6 +24,10 @@ _sz = ctypes.c_size_t
 SIGNATURES = {
     "ddfan_last_error": (ctypes.c_char_p, []),
     "ddfan_version": (_i, []),
+    "ddfan_tune_set_zl": (_i, [_i, _i]),
+    "ddfan_tune_get_zl": (_i, [_i]),
+    "ddfan_plan_estimate_bytes": (_sz, [_i, _i, _i, _i, _i, _i]),
+    "ddfan_ossart_estimate_bytes": (_sz, [_i, _i, _i, _i, _i, _i, _i]),
     "ddfan_fan_geometry": (_i, [_f, _f, _i, _f, _f, _p, _p, _p, _p]),
     "ddfan_MultiSlicesProjGPU": (_i, [_f, _f, _i, _p, _p, _f, _f, _p, _i, _i, _i, _i, _p, _f, _p, _p,
                                       _i, _i, _p]),

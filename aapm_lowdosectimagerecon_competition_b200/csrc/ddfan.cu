@@ -7,6 +7,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -64,11 +65,26 @@ LaunchProfiler::~LaunchProfiler() {
 
 // ------------------------------------------------------------------ plan
 
+// Tile widths chosen by the autotuner (ddfan_tune_set_zl), keyed by the
+// number of 4-slice blocks; consulted before the built-in cost model.
+static std::mutex g_tune_mutex;
+static std::map<int, int> g_tuned_zl;
+
+static int tuned_zl(int ZB) {
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  auto it = g_tuned_zl.find(ZB);
+  return it == g_tuned_zl.end() ? 0 : it->second;
+}
+
 // z-blocks per z-tile: wider tiles gather more contiguous bytes per request,
 // but a stack of ZB blocks is padded to whole tiles.  Relative cost per
 // padded block of each width (measured on the 512^2 x 128 workload: widths
-// 8, 4, 2 ran at 1 : 1.2 : 2.1); pick the cheapest padded stack.
+// 8, 4, 2 ran at 1 : 1.2 : 2.1); pick the cheapest padded stack, unless the
+// autotuner recorded a measured choice for this stack.
 int pow2_zl(int ZB) {
+  const int t = tuned_zl(ZB);
+  if (t == 1 || t == 2 || t == 4 || t == 8)
+    if (t <= ZB) return t;
   const int widths[4] = {8, 4, 2, 1};
   const double cost[4] = {1.0, 1.2, 2.1, 3.6};
   int best = 1;
@@ -82,32 +98,55 @@ int pow2_zl(int ZB) {
   return best;
 }
 
-template <class T>
-static int dalloc(T** p, size_t n, size_t* bytes) {
+// Stream-ordered device memory (cudaMallocAsync / cudaFreeAsync from the
+// device's default pool): creating or destroying a plan or a solver never
+// synchronises the device, so other solves keep running meanwhile.
+int dev_alloc(void** p, size_t bytes, cudaStream_t st) {
   *p = nullptr;
-  if (n == 0) n = 1;
-  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  cudaError_t e = cudaMallocAsync(p, std::max<size_t>(bytes, 1), st);
   if (e != cudaSuccess) {
     *p = nullptr;
     cudaGetLastError();
-    return set_err(DDFAN_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+    return set_err(DDFAN_ERR_NOMEM, "cudaMallocAsync(%zu bytes): %s", bytes, cudaGetErrorString(e));
   }
-  *bytes += n * sizeof(T);
   return DDFAN_OK;
 }
 
+void dev_free(void* p, cudaStream_t st) {
+  if (p) cudaFreeAsync(p, st);
+}
+
+template <class T>
+static int dalloc(T** p, size_t n, size_t* bytes, cudaStream_t st) {
+  if (n == 0) n = 1;
+  int rc = dev_alloc((void**)p, n * sizeof(T), st);
+  if (!rc) *bytes += n * sizeof(T);
+  return rc;
+}
+
+// Releases a plan's device memory once the plan's last recorded use
+// (mark_use) has completed; does not block the host.
 void plan_free(Plan* P) {
   if (!P) return;
   int prev = -1;
   cudaGetDevice(&prev);
   cudaSetDevice(P->device);
-  void* ptrs[] = {P->d_bx, P->d_by, P->d_xd, P->d_yd, P->d_mask, P->d_tb, P->d_lut, P->d_satx,
-                  P->d_saty, P->d_satq, P->d_vg, P->d_fc, P->d_cvd, P->d_tmp, P->d_angs,
-                  P->d_order, P->d_counts};
-  for (void* q : ptrs)
-    if (q) cudaFree(q);
+  if (P->alloc_stream) {
+    if (P->last_use) cudaStreamWaitEvent(P->alloc_stream, P->last_use, 0);
+    void* ptrs[] = {P->d_bx, P->d_by, P->d_xd, P->d_yd, P->d_mask, P->d_tb, P->d_lut, P->d_satx,
+                    P->d_saty, P->d_satq, P->d_vg, P->d_fc, P->d_cvd, P->d_tmp, P->d_angs,
+                    P->d_order, P->d_counts};
+    for (void* q : ptrs) dev_free(q, P->alloc_stream);
+    cudaStreamDestroy(P->alloc_stream);
+  }
+  if (P->last_use) cudaEventDestroy(P->last_use);
+  cudaGetLastError();
   if (prev >= 0) cudaSetDevice(prev);
   delete P;
+}
+
+void mark_use(Plan& p, cudaStream_t st) {
+  if (p.last_use) cudaEventRecord(p.last_use, st);
 }
 
 // DD3Boundaries (AAPM_script/utilities.cuh:268-287): evaluated in double,
@@ -204,19 +243,26 @@ int plan_create(Plan** out, const PlanDesc& d) {
   }
   size_t& B = p.bytes;
   int rc;
+  if (cudaStreamCreateWithFlags(&p.alloc_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&p.last_use, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    if (prev >= 0) cudaSetDevice(prev);
+    return set_err(DDFAN_ERR_CUDA, "plan: stream/event creation failed");
+  }
+  cudaStream_t as = p.alloc_stream;
   const size_t F4 = cell_f4(p.mode);
   const size_t nimg = (size_t)p.XN * p.YN * p.ZB * F4;
   const size_t nsino = (size_t)p.PNmax * (p.U + 1) * p.ZB * F4;
-  if ((rc = dalloc(&p.d_bx, p.U + 1, &B)) || (rc = dalloc(&p.d_by, p.U + 1, &B)) ||
-      (rc = dalloc(&p.d_xd, p.U, &B)) || (rc = dalloc(&p.d_yd, p.U, &B)) ||
-      (rc = dalloc(&p.d_mask, (size_t)p.XN * p.YN, &B)) || (rc = dalloc(&p.d_tb, p.U + 1, &B)) ||
-      (rc = dalloc(&p.d_lut, p.M, &B)) || (rc = dalloc(&p.d_satx, nimg, &B)) ||
-      (rc = dalloc(&p.d_saty, nimg, &B)) || (rc = dalloc(&p.d_satq, nsino, &B)) ||
-      (rc = dalloc(&p.d_vg, p.PNmax, &B)) || (rc = dalloc(&p.d_fc, (size_t)p.PNmax * (p.U + 1), &B)) ||
-      (rc = dalloc(&p.d_cvd, (size_t)p.PNmax * p.U, &B)) ||
-      (rc = dalloc(&p.d_tmp, (size_t)p.XN * p.YN * p.Z, &B)) ||
-      (rc = dalloc(&p.d_angs, (size_t)p.PNmax, &B)) ||
-      (rc = dalloc(&p.d_order, (size_t)p.PNmax, &B)) || (rc = dalloc(&p.d_counts, 2, &B))) {
+  if ((rc = dalloc(&p.d_bx, p.U + 1, &B, as)) || (rc = dalloc(&p.d_by, p.U + 1, &B, as)) ||
+      (rc = dalloc(&p.d_xd, p.U, &B, as)) || (rc = dalloc(&p.d_yd, p.U, &B, as)) ||
+      (rc = dalloc(&p.d_mask, (size_t)p.XN * p.YN, &B, as)) || (rc = dalloc(&p.d_tb, p.U + 1, &B, as)) ||
+      (rc = dalloc(&p.d_lut, p.M, &B, as)) || (rc = dalloc(&p.d_satx, nimg, &B, as)) ||
+      (rc = dalloc(&p.d_saty, nimg, &B, as)) || (rc = dalloc(&p.d_satq, nsino, &B, as)) ||
+      (rc = dalloc(&p.d_vg, p.PNmax, &B, as)) || (rc = dalloc(&p.d_fc, (size_t)p.PNmax * (p.U + 1), &B, as)) ||
+      (rc = dalloc(&p.d_cvd, (size_t)p.PNmax * p.U, &B, as)) ||
+      (rc = dalloc(&p.d_tmp, (size_t)p.XN * p.YN * p.Z, &B, as)) ||
+      (rc = dalloc(&p.d_angs, (size_t)p.PNmax, &B, as)) ||
+      (rc = dalloc(&p.d_order, (size_t)p.PNmax, &B, as)) || (rc = dalloc(&p.d_counts, 2, &B, as))) {
     if (prev >= 0) cudaSetDevice(prev);
     return rc;
   }
@@ -224,14 +270,16 @@ int plan_create(Plan** out, const PlanDesc& d) {
   if (d.mask) std::memcpy(m.data(), d.mask, m.size());
   p.has_mask = d.mask != nullptr;
   cudaError_t e = cudaSuccess;
-  if (e == cudaSuccess) e = cudaMemcpy(p.d_bx, p.bx.data(), sizeof(double) * (p.U + 1), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(p.d_by, p.by.data(), sizeof(double) * (p.U + 1), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(p.d_bx, p.bx.data(), sizeof(double) * (p.U + 1), cudaMemcpyHostToDevice, as);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(p.d_by, p.by.data(), sizeof(double) * (p.U + 1), cudaMemcpyHostToDevice, as);
   std::vector<double> xd(p.xd.begin(), p.xd.end()), yd(p.yd.begin(), p.yd.end());
-  if (e == cudaSuccess) e = cudaMemcpy(p.d_xd, xd.data(), sizeof(double) * p.U, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(p.d_yd, yd.data(), sizeof(double) * p.U, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(p.d_mask, m.data(), m.size(), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(p.d_tb, p.tb.data(), sizeof(float) * (p.U + 1), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(p.d_lut, p.lut.data(), sizeof(uint16_t) * p.M, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(p.d_xd, xd.data(), sizeof(double) * p.U, cudaMemcpyHostToDevice, as);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(p.d_yd, yd.data(), sizeof(double) * p.U, cudaMemcpyHostToDevice, as);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(p.d_mask, m.data(), m.size(), cudaMemcpyHostToDevice, as);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(p.d_tb, p.tb.data(), sizeof(float) * (p.U + 1), cudaMemcpyHostToDevice, as);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(p.d_lut, p.lut.data(), sizeof(uint16_t) * p.M, cudaMemcpyHostToDevice, as);
+  // the allocations and the staged uploads complete before the plan is used on any stream
+  if (e == cudaSuccess) e = cudaStreamSynchronize(as);
   if (prev >= 0) cudaSetDevice(prev);
   if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "plan upload: %s", cudaGetErrorString(e));
   *out = P.release();
@@ -452,7 +500,9 @@ int proj_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const floa
   if ((rc = launch_view_geom(p, d_angs, stride, PN, p.d_vg, p.d_fc, p.d_cvd, st))) return rc;
   if ((rc = launch_view_order(p.d_vg, PN, p.d_order, p.d_counts, st))) return rc;
   if ((rc = launch_sat_image(p, d_vol, st))) return rc;
-  return launch_fwd(p, p.d_vg, p.d_fc, p.d_cvd, p.d_order, PN, d_prj, zlo, zhi, st);
+  rc = launch_fwd(p, p.d_vg, p.d_fc, p.d_cvd, p.d_order, PN, d_prj, zlo, zhi, st);
+  mark_use(p, st);
+  return rc;
 }
 
 int back_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const float* d_prj, float* d_vol,
@@ -465,7 +515,9 @@ int back_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const floa
     return rc;
   BackEpi e{};
   e.out = d_vol; e.mask = p.has_mask ? p.d_mask : nullptr; e.zlo = zlo; e.zhi = zhi;
-  return launch_back(p, back_mode, p.d_vg, p.d_fc, p.d_order, p.d_counts, PN, e, st);
+  rc = launch_back(p, back_mode, p.d_vg, p.d_fc, p.d_order, p.d_counts, PN, e, st);
+  mark_use(p, st);
+  return rc;
 }
 
 // Groups of slices sharing one angle list: per-slice angle arrays
@@ -528,6 +580,30 @@ extern "C" {
 
 DDFAN_API const char* ddfan_last_error(void) { return ddfan::last_error(); }
 DDFAN_API int ddfan_version(void) { return 1; }
+
+DDFAN_API int ddfan_tune_set_zl(int zblocks, int zl) {
+  if (zblocks < 1 || !(zl == 0 || zl == 1 || zl == 2 || zl == 4 || zl == 8) || zl > zblocks)
+    return set_err(DDFAN_ERR_ARG, "tune_set_zl: zblocks=%d zl=%d", zblocks, zl);
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  if (zl == 0) g_tuned_zl.erase(zblocks);
+  else g_tuned_zl[zblocks] = zl;
+  return DDFAN_OK;
+}
+
+DDFAN_API int ddfan_tune_get_zl(int zblocks) { return zblocks < 1 ? 0 : pow2_zl(zblocks); }
+
+DDFAN_API size_t ddfan_plan_estimate_bytes(int XN, int YN, int DNU, int SLN, int PNmax, int sat_mode) {
+  if (XN < 1 || YN < 1 || DNU < 2 || SLN < 1 || PNmax < 1 || sat_mode < 0 || sat_mode > 2) return 0;
+  int ZB = (SLN + 3) / 4;
+  const int ZL = pow2_zl(ZB);
+  ZB = (ZB + ZL - 1) / ZL * ZL;
+  const size_t F4 = cell_f4(sat_mode), U = (size_t)DNU, P = (size_t)PNmax;
+  const size_t cells = 2 * (size_t)XN * YN * ZB * F4 + P * (U + 1) * ZB * F4;
+  return cells * sizeof(float4) + (2 * (U + 1) + 2 * U) * sizeof(double) + (size_t)XN * YN +
+         (U + 1) * sizeof(float) + 4 * (U + 1) * sizeof(uint16_t) + P * sizeof(ViewGeom) +
+         P * (U + 1) * sizeof(double2) + P * U * sizeof(float) + (size_t)XN * YN * SLN * sizeof(float) +
+         P * sizeof(float) + P * sizeof(int) + 2 * sizeof(int);
+}
 
 DDFAN_API int ddfan_fan_geometry(float sid, float sdd, int DNU, float detCellWidth, float detCntIdx,
                                  float* x0, float* y0, float* xds, float* yds) {

@@ -53,10 +53,17 @@ struct Plan {
   float* d_angs = nullptr;  // PNmax angles (host-angle entry points)
   int* d_order = nullptr;   // PNmax views in dispatch order (x-major first)
   int* d_counts = nullptr;  // {x-major views, others}
+  cudaStream_t alloc_stream = nullptr;  // stream-ordered allocation / release
+  cudaEvent_t last_use = nullptr;       // recorded after every call's launches
   size_t bytes = 0;
 };
 
 int plan_create(Plan** out, const PlanDesc& d);
+// stream-ordered device allocation (never synchronises the device)
+int dev_alloc(void** p, size_t bytes, cudaStream_t st);
+void dev_free(void* p, cudaStream_t st);
+// records the plan's last use on `st`; plan_free releases memory after it
+void mark_use(Plan& p, cudaStream_t st);
 // z-blocks per z-tile for a stack of ZB 4-slice blocks
 int pow2_zl(int ZB);
 // DD3Boundaries (AAPM_script/utilities.cuh:268-287), float-rounded like the reference stores them

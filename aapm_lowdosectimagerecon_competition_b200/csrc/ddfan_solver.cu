@@ -24,18 +24,10 @@ struct PlanPtr {
 template <class T>
 struct DevBuf {
   T* p = nullptr;
-  ~DevBuf() {
-    if (p) cudaFree(p);
-  }
-  int alloc(size_t n) {
-    cudaError_t e = cudaMalloc((void**)&p, std::max<size_t>(n, 1) * sizeof(T));
-    if (e != cudaSuccess) {
-      p = nullptr;
-      cudaGetLastError();
-      return set_err(DDFAN_ERR_NOMEM, "cudaMalloc(%zu): %s", n * sizeof(T), cudaGetErrorString(e));
-    }
-    return DDFAN_OK;
-  }
+  cudaStream_t st = nullptr;  // allocation and release are ordered on this stream
+  explicit DevBuf(cudaStream_t s = nullptr) : st(s) {}
+  ~DevBuf() { dev_free(p, st); }
+  int alloc(size_t n) { return dev_alloc((void**)&p, std::max<size_t>(n, 1) * sizeof(T), st); }
 };
 
 #define DDFAN_CK(call)                                                                         \
@@ -184,6 +176,7 @@ struct Solver {
   float* d_ax = nullptr;   // [PNmax][U][Z]
   double* d_t = nullptr;
   cudaStream_t own = nullptr;
+  cudaEvent_t last_use = nullptr;  // recorded after work enqueued on a caller's stream
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   size_t bytes = 0;
@@ -195,13 +188,20 @@ static void solver_free(Solver* s) {
   int prev = -1;
   cudaGetDevice(&prev);
   cudaSetDevice(s->device);
+  // release after the solver's last use (possibly on a caller's stream),
+  // without synchronising the rest of the device
+  if (s->own && s->last_use) {
+    cudaStreamWaitEvent(s->own, s->last_use, 0);
+    cudaStreamSynchronize(s->own);
+  }
   if (s->gexec) cudaGraphExecDestroy(s->gexec);
   if (s->graph) cudaGraphDestroy(s->graph);
-  if (s->own) cudaStreamDestroy(s->own);
   void* ptrs[] = {s->d_vg, s->d_fc, s->d_cvd, s->d_yview, s->d_order, s->d_counts, s->d_rows, s->d_cols,
                   s->d_y, s->d_x, s->d_xprev, s->d_ax, s->d_t};
-  for (void* q : ptrs)
-    if (q) cudaFree(q);
+  for (void* q : ptrs) dev_free(q, s->own);
+  if (s->own) cudaStreamDestroy(s->own);
+  if (s->last_use) cudaEventDestroy(s->last_use);
+  cudaGetLastError();
   plan_free(s->P);
   if (prev >= 0) cudaSetDevice(prev);
   delete s;
@@ -209,14 +209,9 @@ static void solver_free(Solver* s) {
 
 template <class T>
 static int salloc(Solver& s, T** p, size_t n) {
-  cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T));
-  if (e != cudaSuccess) {
-    *p = nullptr;
-    cudaGetLastError();
-    return set_err(DDFAN_ERR_NOMEM, "solver cudaMalloc(%zu): %s", n * sizeof(T), cudaGetErrorString(e));
-  }
-  s.bytes += std::max<size_t>(n, 1) * sizeof(T);
-  return DDFAN_OK;
+  const int rc = dev_alloc((void**)p, std::max<size_t>(n, 1) * sizeof(T), s.own);
+  if (!rc) s.bytes += std::max<size_t>(n, 1) * sizeof(T);
+  return rc;
 }
 
 // One OS-SART iteration (AAPM_script/OSSART_AAPM.m:79-115) on stream st.
@@ -296,6 +291,8 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
   s.bytes = s.P->bytes;
   DeviceGuard g(device);
   const size_t V = (size_t)XN * YN * SLN;
+  DDFAN_CK(cudaStreamCreateWithFlags(&s.own, cudaStreamNonBlocking));
+  DDFAN_CK(cudaEventCreateWithFlags(&s.last_use, cudaEventDisableTiming));
   if ((rc = salloc(s, &s.d_vg, PNall)) || (rc = salloc(s, &s.d_fc, (size_t)PNall * (DNU + 1))) ||
       (rc = salloc(s, &s.d_cvd, (size_t)PNall * DNU)) || (rc = salloc(s, &s.d_yview, PNall)) ||
       (rc = salloc(s, &s.d_order, PNall)) || (rc = salloc(s, &s.d_counts, 2 * (size_t)numOfOS)) || (rc = salloc(s, &s.d_rows, (size_t)PNall * DNU)) ||
@@ -304,10 +301,9 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
       (rc = salloc(s, &s.d_xprev, V)) || (rc = salloc(s, &s.d_ax, (size_t)PNmax * DNU * SLN)) ||
       (rc = salloc(s, &s.d_t, 1)))
     return rc;
-  DDFAN_CK(cudaStreamCreateWithFlags(&s.own, cudaStreamNonBlocking));
   cudaStream_t st = s.own;
   // per-view tables for every view, in subset order
-  DevBuf<float> dang;
+  DevBuf<float> dang(st);
   if ((rc = dang.alloc(PNall))) return rc;
   DDFAN_CK(cudaMemcpyAsync(dang.p, angs.data(), sizeof(float) * PNall, cudaMemcpyHostToDevice, st));
   DDFAN_CK(cudaMemcpyAsync(s.d_yview, yview.data(), sizeof(int) * PNall, cudaMemcpyHostToDevice, st));
@@ -323,7 +319,7 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
     d1.SLN = 1;
     PlanPtr P1;
     if ((rc = plan_create(&P1.p, d1))) return rc;
-    DevBuf<float> ones, tmp;
+    DevBuf<float> ones(st), tmp(st);
     const size_t n1 = std::max((size_t)XN * YN, (size_t)PNmax * DNU);
     if ((rc = ones.alloc(n1)) || (rc = tmp.alloc((size_t)PNmax * DNU))) return rc;
     std::vector<float> h1(n1, 1.0f);
@@ -402,6 +398,23 @@ DDFAN_API int ddfan_ossart_create(ddfan_ossart** out, float x0, float y0, int DN
 
 DDFAN_API void ddfan_ossart_destroy(ddfan_ossart* s) { solver_free(reinterpret_cast<Solver*>(s)); }
 
+DDFAN_API size_t ddfan_ossart_estimate_bytes(int XN, int YN, int DNU, int SLN, int PNall, int numOfOS,
+                                             int sat_mode) {
+  if (numOfOS < 1 || PNall < numOfOS) return 0;
+  const size_t PNmax = (size_t)(PNall + numOfOS - 1) / numOfOS;
+  const size_t U = (size_t)DNU, P = (size_t)PNall, V = (size_t)XN * YN * SLN;
+  const size_t plan = ddfan_plan_estimate_bytes(XN, YN, DNU, SLN, (int)PNmax, sat_mode);
+  if (!plan) return 0;
+  const size_t own = P * sizeof(ViewGeom) + P * (U + 1) * sizeof(double2) + P * U * sizeof(float) +
+                     3 * P * sizeof(int) + 2 * (size_t)numOfOS * sizeof(int) + P * U * sizeof(float) +
+                     (size_t)numOfOS * XN * YN * sizeof(float) + P * U * SLN * sizeof(float) +
+                     2 * V * sizeof(float) + PNmax * U * SLN * sizeof(float) + sizeof(double);
+  // transient at creation: the one-slice weight plan and its buffers
+  const size_t weights = ddfan_plan_estimate_bytes(XN, YN, DNU, 1, (int)PNmax, sat_mode) +
+                         (std::max((size_t)XN * YN, PNmax * U) + PNmax * U + P) * sizeof(float);
+  return plan + own + weights;
+}
+
 DDFAN_API size_t ddfan_ossart_device_bytes(const ddfan_ossart* s) {
   return s ? reinterpret_cast<const Solver*>(s)->bytes : 0;
 }
@@ -414,6 +427,7 @@ DDFAN_API int ddfan_ossart_set_sinogram(ddfan_ossart* h, const float* proj, int 
   DDFAN_CK(cudaMemcpyAsync(s->d_y, proj, sizeof(float) * n,
                            is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                            (cudaStream_t)stream));
+  cudaEventRecord(s->last_use, (cudaStream_t)stream);
   return DDFAN_OK;
 }
 
@@ -443,6 +457,7 @@ DDFAN_API int ddfan_ossart_iterate(ddfan_ossart* h, int numOfIter, int use_graph
       int rc = solver_iteration(*s, st);
       if (rc) return rc;
     }
+    cudaEventRecord(s->last_use, st);
     return DDFAN_OK;
   }
   if (!s->gexec) {
@@ -459,6 +474,7 @@ DDFAN_API int ddfan_ossart_iterate(ddfan_ossart* h, int numOfIter, int use_graph
     DDFAN_CK(cudaGraphInstantiate(&s->gexec, s->graph, 0));
   }
   for (int it = 0; it < numOfIter; ++it) DDFAN_CK(cudaGraphLaunch(s->gexec, st));
+  cudaEventRecord(s->last_use, st);
   return DDFAN_OK;
 }
 
@@ -470,6 +486,7 @@ DDFAN_API int ddfan_ossart_get_image(ddfan_ossart* h, float* img, int is_device,
   cudaStream_t st = (cudaStream_t)stream;
   DDFAN_CK(cudaMemcpyAsync(img, s->d_x, sizeof(float) * n,
                            is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+  cudaEventRecord(s->last_use, st);
   if (!is_device) DDFAN_CK(cudaStreamSynchronize(st));
   return DDFAN_OK;
 }

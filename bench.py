@@ -47,7 +47,84 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--kernels", action="store_true",
                     help="time only one subset's projector kernels (small case for ncu captures)")
+    ap.add_argument("--config", default="c3", choices=["c3", "c4", "c5"],
+                    help="c3: the OS-SART contract line; c4: batched uneven reconstructions; "
+                         "c5: Poisson-arrival serving")
+    ap.add_argument("--instances", type=int, default=32)
+    ap.add_argument("--window", type=float, default=20.0)
+    ap.add_argument("--rate", type=float, default=20.0)
     return ap.parse_args()
+
+
+def _c4_instances(args, dev, iters):
+    from aapm_lowdosectimagerecon_competition_b200 import configs, serve
+    sizes = configs.c4_instances(args.instances)
+    tuner = serve.TileTuner(sat=args.sat)
+    for zb in sorted({(Z + 3) // 4 for _, Z, _ in sizes}):
+        tuner.tune(N=512, Z=4 * zb, P=96, device=dev, reps=1)
+    insts = [serve.make_instance(N, Z, P, seed=100 + i, device=dev, iters=iters)
+             for i, (N, Z, P) in enumerate(sizes)]
+    return insts, tuner
+
+
+def run_c4(args):
+    """Config 4: 32 seeded instances (side 256-768, 8-96 slices, 720-2304 views,
+    736 channels), 5 OS-SART iterations each, hi/lo prefix sums, tile widths
+    from the autotuner.  All submitted at once; the engine runs up to 8 solves
+    concurrently (each a CUDA-graph replay per iteration on its own stream)
+    and is compared with the same instances one at a time."""
+    import torch
+    from aapm_lowdosectimagerecon_competition_b200 import serve
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    insts, tuner = _c4_instances(args, dev, iters=5)
+    res = {}
+    for name, k in (("serial", 1), ("batched", 8)):
+        eng = serve.Engine(device=0, max_active=k, sat=args.sat, back=args.back)
+        res[name] = serve.run_batch(insts, eng)
+    line = {"metric": "c4 batched OS-SART iterations/s (32 uneven instances, 5 iterations each)",
+            "value": res["batched"]["iters_per_s"], "unit": "iter/s", "higher_is_better": True,
+            "batched": res["batched"], "serial": res["serial"],
+            "speedup_vs_serial": res["batched"]["iters_per_s"] / res["serial"]["iters_per_s"],
+            "tile_table": tuner.table, "sat": args.sat, "back": args.back, "data": "synthetic"}
+    print(json.dumps(line), flush=True)
+
+
+def run_c5(args):
+    """Config 5: Poisson arrivals at --rate requests/s of config-4-sized
+    requests, 10 OS-SART iterations each, 150 GB admission budget, for a
+    --window seconds wall-clock window; compared with serial plain-FP32
+    solves (FP32 prefix sums, reference backprojector, no graphs, one at a
+    time) of requests from the same pool."""
+    import torch
+    from aapm_lowdosectimagerecon_competition_b200 import serve
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    args.instances = min(args.instances, 8)
+    pool, tuner = _c4_instances(args, dev, iters=10)
+    eng = serve.Engine(device=0, budget_bytes=150e9, max_active=8, sat=args.sat, back=args.back)
+    served = serve.run_serving(pool, eng, rate_hz=args.rate, window_s=args.window)
+    # serial plain FP32, mex-style (host round trips per subset), one iteration of
+    # two pool requests timed and scaled to the pool's mean work per request
+    mex_rate = []
+    for inst in pool[:2]:
+        sec = serve.plain_mex_seconds_per_iter(inst.scan, inst.proj_host.numpy(), inst.mask)
+        mex_rate.append(inst.work / sec)
+    mex_samples = float(np.mean(mex_rate))
+    # serial device-resident solves with FP32 sums and the reference backprojector, no graphs
+    plain = serve.Engine(device=0, max_active=1, sat="fp32", back="ref", use_graph=False)
+    pb = serve.run_batch(pool, plain)
+    line = {"metric": "c5 served OS-SART requests/s (Poisson %.0f req/s, 10 iterations each)" % args.rate,
+            "value": served["served_rate_hz"], "unit": "req/s", "higher_is_better": True,
+            "serving": served,
+            "serial_plain_fp32_mex": {"samples_per_s": mex_samples,
+                                      "req_per_s": mex_samples / (10 * np.mean([i.work for i in pool]))},
+            "serial_device_fp32_ref": {"req_per_s": pb["instances"] / pb["wall_s"],
+                                       "iters_per_s": pb["iters_per_s"], "samples_per_s": pb["samples_per_s"]},
+            "throughput_vs_serial_plain_mex": served["samples_per_s"] / mex_samples,
+            "throughput_vs_serial_device_fp32": served["samples_per_s"] / pb["samples_per_s"],
+            "budget_gb": 150, "data": "synthetic"}
+    print(json.dumps(line), flush=True)
 
 
 def run_kernels(args):
@@ -368,39 +445,10 @@ def _ossart_host(s, geom, y_h, x_h, out_h, mask, iters, args):
 
 
 def plain_fp32_iteration(s, geom, y, mask):
-    """One OS-SART iteration executed the way AAPM_script/OSSART_AAPM.m drives
-    the mex functions: per subset a host-pointer projection call, the residual
-    on the host, a host-pointer backprojection call, the update on the host;
-    FP32 prefix sums, reference backprojector, no graphs."""
-    from aapm_lowdosectimagerecon_competition_b200 import dd2
-    x0, y0, xds, yds = geom
-    yh = y.cpu().numpy()
-    hangs = s.hangs()
-    x = np.zeros((s.YN, s.XN, s.SLN), np.float32)
-    ones_i = np.ones((s.YN, s.XN, 1), np.float32)
-    subs = [np.arange(k, s.PN, s.numOfOS) for k in range(s.numOfOS)]
-    rows, cols = [], []
-    for v in subs:
-        h1 = np.ascontiguousarray(hangs[v][:, :1])
-        rows.append(dd2.MultiSlicesProjGPU(x0, y0, s.DNU, xds, yds, 0, 0, h1, len(v), s.XN, s.YN, 1,
-                                           ones_i, s.dx, mask, sat="fp32"))
-        cols.append(dd2.MultiSlicesBackGPU(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0, 0, h1, len(v),
-                                           s.XN, s.YN, 1, np.ones((len(v), s.DNU, 1), np.float32), s.dx,
-                                           mask, sat="fp32", back="ref"))
-    t0 = time.perf_counter()
-    for k, v in enumerate(subs):
-        h = np.ascontiguousarray(hangs[v])
-        prj = dd2.MultiSlicesProjGPU(x0, y0, s.DNU, xds, yds, 0, 0, h, len(v), s.XN, s.YN, s.SLN, x,
-                                     s.dx, mask, sat="fp32")
-        rs = rows[k]
-        nz = np.broadcast_to(rs != 0, prj.shape)
-        prj = np.where(nz, (yh[v] - prj) / np.where(rs != 0, rs, 1), prj).astype(np.float32)
-        tp = dd2.MultiSlicesBackGPU(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0, 0, h, len(v), s.XN, s.YN,
-                                    s.SLN, prj, s.dx, mask, sat="fp32", back="ref")
-        cs = cols[k]
-        tp = np.where(np.broadcast_to(cs != 0, tp.shape), tp / np.where(cs != 0, cs, 1), tp)
-        x = np.maximum(x + tp, 0).astype(np.float32)
-    sec = time.perf_counter() - t0
+    """One OS-SART iteration the way AAPM_script/OSSART_AAPM.m drives the mex
+    functions (serve.plain_mex_seconds_per_iter)."""
+    from aapm_lowdosectimagerecon_competition_b200 import serve
+    sec = serve.plain_mex_seconds_per_iter(s, y.cpu().numpy(), mask)
     return {"value": 1.0 / sec, "unit": UNIT, "seconds_per_iter": sec,
             "how": "mex-style: per subset host->device image, FP32 prefix sums, forward, "
                    "device->host sinogram, host residual, host->device, REF backprojection, "
@@ -413,6 +461,10 @@ def main():
         run_reference(args)
     elif args.kernels:
         run_kernels(args)
+    elif args.config == "c4":
+        run_c4(args)
+    elif args.config == "c5":
+        run_c5(args)
     else:
         run_ours(args)
 

@@ -50,6 +50,20 @@ extern "C" {
 DDFAN_API const char* ddfan_last_error(void);
 DDFAN_API int ddfan_version(void);
 
+/* ---- tile selection and memory estimates (serving / autotuning) ----
+ * No counterpart in the reference.  Plans split the slices into z-tiles of
+ * zl 4-slice blocks (zl in {1, 2, 4, 8}); by default a cost model picks zl
+ * for a stack of `zblocks` blocks, ddfan_tune_set_zl records a measured
+ * choice (zl = 0 forgets it).  Process-wide, thread-safe; affects plans
+ * created afterwards. */
+DDFAN_API int ddfan_tune_set_zl(int zblocks, int zl);
+DDFAN_API int ddfan_tune_get_zl(int zblocks);
+/* device bytes ddfan_plan_create / ddfan_ossart_create would allocate
+ * (the solver figure includes its transient set-up buffers); 0 = bad sizes */
+DDFAN_API size_t ddfan_plan_estimate_bytes(int XN, int YN, int DNU, int SLN, int PNmax, int sat_mode);
+DDFAN_API size_t ddfan_ossart_estimate_bytes(int XN, int YN, int DNU, int SLN, int PNall, int numOfOS,
+                                             int sat_mode);
+
 /* Source position and channel centres on the arc detector, as the MATLAB
  * wrapper builds them (replaces AAPM_script/DD2MutiSlices.m:49-76):
  * stepTheta = 2 atan(detCellWidth / 2 / sdd), beta_i = (i - detCntIdx) stepTheta
