@@ -316,11 +316,12 @@ static int sat_dispatch(const SatSrc& s, float4* out0, int nl0, float4* out1, in
                         int Nw0, int Nw1, int ZB, int ntab, cudaStream_t st) {
   const int Nw = std::max(Nw0, Nw1);
   dim3 grid(std::max(nl0, nl1), (ZB + 7) / 8, ntab);
-  if (Nw <= 32 * 4) k_sat<M, 4><<<grid, 256, 0, st>>>(s, out0, nl0, nl1, out1, N0, N1, Nw0, Nw1, ZB);
-  else if (Nw <= 32 * 8) k_sat<M, 8><<<grid, 256, 0, st>>>(s, out0, nl0, nl1, out1, N0, N1, Nw0, Nw1, ZB);
-  else if (Nw <= 32 * 16) k_sat<M, 16><<<grid, 256, 0, st>>>(s, out0, nl0, nl1, out1, N0, N1, Nw0, Nw1, ZB);
-  else if (Nw <= 32 * 24) k_sat<M, 24><<<grid, 256, 0, st>>>(s, out0, nl0, nl1, out1, N0, N1, Nw0, Nw1, ZB);
-  else if (Nw <= 32 * 32) k_sat<M, 32><<<grid, 256, 0, st>>>(s, out0, nl0, nl1, out1, N0, N1, Nw0, Nw1, ZB);
+  // 512 threads = 8 z lanes x 64 chunks of C cells
+  if (Nw <= 64 * 2) k_sat<M, 2><<<grid, 512, 0, st>>>(s, out0, nl0, nl1, out1, N0, N1, Nw0, Nw1, ZB);
+  else if (Nw <= 64 * 4) k_sat<M, 4><<<grid, 512, 0, st>>>(s, out0, nl0, nl1, out1, N0, N1, Nw0, Nw1, ZB);
+  else if (Nw <= 64 * 8) k_sat<M, 8><<<grid, 512, 0, st>>>(s, out0, nl0, nl1, out1, N0, N1, Nw0, Nw1, ZB);
+  else if (Nw <= 64 * 12) k_sat<M, 12><<<grid, 512, 0, st>>>(s, out0, nl0, nl1, out1, N0, N1, Nw0, Nw1, ZB);
+  else if (Nw <= 64 * 16) k_sat<M, 16><<<grid, 512, 0, st>>>(s, out0, nl0, nl1, out1, N0, N1, Nw0, Nw1, ZB);
   else return set_err(DDFAN_ERR_UNSUPPORTED, "line of %d cells", Nw);
   return check_launch("k_sat");
 }

@@ -145,15 +145,16 @@ __device__ __forceinline__ void sat_load(const SatSrc& s, int line, int k, int z
   for (int i = 0; i < 4; ++i) v[i] *= m;
 }
 
-// Prefix sums along every line: one CTA per (line, 32-slice tile), 256 threads.
+// Prefix sums along every line: one CTA per (line, 32-slice tile), 512 threads.
 // Thread (zl = tid % 8, kc = tid / 8) owns 4 slices and the chunk
-// [kc*C, kc*C + C) of the line.  Chunk sums are combined by a warp-shuffle
-// scan across the 4 chunk groups of a warp, then across the 8 warps through
-// shared memory; every thread then writes its chunk's cells.  The inputs stay
-// in registers between the two phases, so each value is read once.
+// [kc*C, kc*C + C) of the line (64 chunks).  Chunk sums are combined by a
+// warp-shuffle scan across the 4 chunk groups of a warp, then across the 16
+// warps through shared memory; every thread then writes its chunk's cells.
+// The inputs stay in registers between the two phases, so each value is read
+// once.
 // Writes Nw >= N cells per line (cells past the last value hold the total).
 template <int M, int C>
-__global__ void __launch_bounds__(256) k_sat(SatSrc s, float4* __restrict__ out, int nlines0,
+__global__ void __launch_bounds__(512) k_sat(SatSrc s, float4* __restrict__ out, int nlines0,
                                              int nlines1, float4* __restrict__ out1, int N0,
                                              int N1, int Nw0, int Nw1, int ZB) {
   constexpr int F4 = CellInfo<M>::F4;
@@ -186,7 +187,7 @@ __global__ void __launch_bounds__(256) k_sat(SatSrc s, float4* __restrict__ out,
   }
   Acc4<M> exc = inc.shfl_up(8);
   if (lane < 8) exc.zero();
-  __shared__ Acc4<M> wtot[8][8];
+  __shared__ Acc4<M> wtot[16][8];  // [warp][z lane]: up to 512 threads
   if (lane >= 24) wtot[w][zl] = inc;
   __syncthreads();
   Acc4<M> run;

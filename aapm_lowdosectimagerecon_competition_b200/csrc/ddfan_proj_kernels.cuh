@@ -219,6 +219,10 @@ struct BackTile {
   static constexpr int LT = NG / SPL;       // lines per tile
   static constexpr int NV = LT * KT;        // voxels per tile
   static constexpr int NE = LT * (KT + 1);  // pixel edges per tile (exact adjoint)
+  // shared-memory layout of a line's edges: one pad slot after every VG edges,
+  // so the VG-edge runs of adjacent groups start 72 bytes apart (no bank conflicts)
+  static constexpr int LS = KT + KT / VG + 1;
+  static constexpr int NES = LT * LS;
 };
 
 struct RefArgs {
@@ -236,7 +240,7 @@ struct RefArgs {
 // (voxel, view) of the tile; phase A differences the two samples of the
 // channel prefix sums in table precision.  Lines are image rows (k = x).
 template <int M, int ZL>
-__global__ void __launch_bounds__(256) k_back_ref(RefArgs a) {
+__global__ void __launch_bounds__(256, 3) k_back_ref(RefArgs a) {
   using T = BackTile<ZL>;
   constexpr int F4 = CellInfo<M>::F4;
   constexpr int NT = T::NT, VG = T::VG, SPL = T::SPL, KT = T::KT, LT = T::LT, NV = T::NV;
@@ -343,13 +347,14 @@ struct AdjArgs {
 // consecutive pixels of a line (VG + 1 edges) x 4 slices.  XM selects the
 // lines (x columns for x-major views, y rows otherwise) and the views.
 template <int M, int ZL, bool XM>
-__global__ void __launch_bounds__(256) k_back_adj(AdjArgs a) {
+__global__ void __launch_bounds__(256, 4) k_back_adj(AdjArgs a) {
   using T = BackTile<ZL>;
   constexpr int F4 = CellInfo<M>::F4;
   constexpr int NT = T::NT, VG = T::VG, SPL = T::SPL, KT = T::KT, LT = T::LT, NE = T::NE;
+  constexpr int LS = T::LS, NES = T::NES;
   constexpr int VC = (1024 / NE) < 1 ? 1 : ((1024 / NE) > 4 ? 4 : 1024 / NE);
   constexpr int TBMAX = 1024, LUTMAX = 4096;
-  __shared__ int2 s_geo[VC][NE];
+  __shared__ int2 s_geo[VC][NES];  // edge k of line l at l * LS + k + k / VG
   __shared__ int s_p[VC];
   __shared__ float s_sgn[VC];
   __shared__ float s_tb[TBMAX];
@@ -414,14 +419,15 @@ __global__ void __launch_bounds__(256) k_back_adj(AdjArgs a) {
           frac = fminf(fmaxf(frac, 0.f), 1.f);
         }
       }
-      s_geo[vv][r] = make_int2(b, __float_as_int(frac));
+      s_geo[vv][le * LS + ke + ke / VG] = make_int2(b, __float_as_int(frac));
     }
     __syncthreads();
     if (active) {
       for (int vv = 0; vv < nvc; ++vv) {
         const float4* base = a.satq + ((size_t)s_p[vv] * (a.U + 1) * a.ZB + blockIdx.z * ZL) * F4 + zl;
         const float sgn = s_sgn[vv];
-        const int2* geo = &s_geo[vv][l * (KT + 1) + sg * VG];
+        // edges sg*VG .. sg*VG + VG of line l (the last one sits after a pad slot)
+        const int2* geo = &s_geo[vv][l * LS + sg * (VG + 1)];
         Phi4<M> prev;
         {
           const int2 gi = geo[0];
@@ -429,7 +435,7 @@ __global__ void __launch_bounds__(256) k_back_adj(AdjArgs a) {
         }
 #pragma unroll
         for (int v = 0; v < VG; ++v) {
-          const int2 gi = geo[v + 1];
+          const int2 gi = geo[v + 1 == VG ? VG + 1 : v + 1];
           Phi4<M> cur;
           cur.load(base + (size_t)gi.x * rowstride, ZL, __int_as_float(gi.y));
           float d[4];

@@ -277,6 +277,26 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+PROFILE_OF = {"fwd": "k_fwd_c3_subset.md", "back_a": "k_back_adj_c3_subset.md",
+              "back_b": "k_back_adj_c3_subset.md"}
+
+
+def profiled_traffic(kernel):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
+    recorded from an ncu capture of this kernel in profiles/, or None."""
+    name = PROFILE_OF.get(kernel)
+    if not name:
+        return None
+    try:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -369,7 +389,8 @@ def run_ours(args):
     peak, peak_kind = peaks()
     achieved = alg[top] / (top_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": profiled_traffic(top), "algorithmic_bytes": alg[top],
                 "launch_ms": top_ms,
                 "kernel_ms_per_iter": {k: round(v[0], 3) for k, v in prof.items()},
                 "note": "achieved = algorithmic bytes per launch / CUDA-event launch time; the "
