@@ -19,6 +19,7 @@ _f = ctypes.c_float
 _i = ctypes.c_int
 _p = ctypes.c_void_p
 _sz = ctypes.c_size_t
+_ll = ctypes.c_longlong
 
 # name -> (restype, argtypes); mirrors include/ddfan.h
 SIGNATURES = {
@@ -52,6 +53,9 @@ SIGNATURES = {
     "ddfan_ossart_profile": (_i, [_p, _i, _p, _p, _p]),
     "ddfan_OSSART_AAPM": (_i, [_f, _f, _i, _p, _p, _f, _f, _f, _p, _p, _i, _i, _i, _i, _f, _p, _p, _i,
                                _i, _i, _i, _i, _i, _p]),
+    "ddfan_HelicalToFan": (_i, [_p, _p, _p, _ll, _p, _i, _f, _f, _f, _i, _i, _f, _f, _i, _f, _f]),
+    "ddfan_helical_to_fan_dev": (_i, [_p, _ll, _p, _i, _f, _f, _f, _i, _i, _f, _f, _i, _f, _f, _i, _p, _p,
+                                      _p]),
 }
 
 _LIB = None

@@ -10,7 +10,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libddfan.so")
-SOURCES = ["ddfan.cu", "ddfan_solver.cu", "ddfan_noalloc.cu"]
+SOURCES = ["ddfan.cu", "ddfan_solver.cu", "ddfan_noalloc.cu", "ddfan_rebin.cu"]
 HEADERS = ["ddfan_device.cuh", "ddfan_kernels.cuh", "ddfan_proj_kernels.cuh", "ddfan_plan.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

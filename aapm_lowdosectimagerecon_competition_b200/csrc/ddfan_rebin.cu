@@ -1,0 +1,348 @@
+// ddfan_rebin.cu -- helical-to-fan single-slice rebinning on the GPU.
+//
+// Same result, bit for bit, as the reference's CPU rebinning HelicalToFanImpl
+// (AAPM_script/HelicalToFanFunc_mex.cpp:41-139, constants :160-164): for every
+// target slice z and view ibeta of one rotation, raw helical view
+// i = start + ibeta - 1 (start = floor((z - h/2) / deltaZ)) is interpolated
+// linearly between detector rows at the row where the fan ray of channel j
+// meets z, weighted by cos of the cone angle; a view any of whose channels
+// falls outside the detector rows is zeroed whole.  Every floating-point
+// operation of the reference is issued as one correctly rounded operation in
+// the same order (no contraction into FMA), and the per-channel constants
+// that the reference takes from the C library (cosf, atanf) are computed on
+// the host with those same functions.
+//
+// Row validity without a reduction: within one output row (slice, view) the
+// only channel-dependent input is SM_j = SO cos(angle_j) > 0, and every
+// operation from SM_j to the interpolation row index is monotone, so the row
+// is valid iff the channels with the smallest and the largest SM_j are.  The
+// kernels evaluate those two once per row.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "ddfan.h"
+#include "ddfan_plan.h"
+
+namespace ddfan {
+namespace {
+
+struct RebinParams {
+  const float* raw;    // raw views [view][W][H]; raw[0] is 1-based raw view view0
+  long long view0;
+  const float* sm;     // [W] SO * cosf((j - DetCenterW) * PerDetA), j 1-based
+  const float* zpos;   // [SLN]
+  const int* start;    // [SLN] floor((z - h/2) / deltaZ)
+  float* out;
+  float* views;
+  int SLN, T, W, H;    // T = DefTimes
+  float SD, SD2, PH, DCH, deltaZ, delta, BV, twopi, sm_lo, sm_hi;
+};
+
+// fractional detector row of the ray with SM at height offset n (1-based, as the reference)
+__device__ __forceinline__ float rebin_dv(const RebinParams& p, float n, float sm, float* v) {
+  const float tanv = __fdiv_rn(n, sm);
+  *v = __fmul_rn(p.SD, tanv);
+  return __fadd_rn(__fdiv_rn(__fadd_rn(p.DCH, *v), p.PH), 1.0f);
+}
+
+__device__ __forceinline__ bool rebin_in_rows(const RebinParams& p, float dv) {
+  return dv >= 1.0f && dv < (float)p.H;  // 1 <= floor(dv) <= H - 1
+}
+
+struct RebinRow {
+  const float* col;  // raw view of this row, channel 0
+  float n;           // z - zz
+  bool ok;           // computed and every channel inside the detector rows
+};
+
+__device__ __forceinline__ RebinRow rebin_row(const RebinParams& p, int s, int ib) {
+  RebinRow r;
+  r.col = nullptr;
+  r.n = 0.f;
+  r.ok = false;
+  const int st = p.start[s];
+  const long long i = (long long)st + ib;  // 1-based raw view
+  if (st < 0 || i < 1) return r;           // the reference's size_t loop skips these
+  const float zz = __fmul_rn((float)(i - 1), p.deltaZ);
+  r.n = __fsub_rn(p.zpos[s], zz);
+  float v;
+  r.ok = rebin_in_rows(p, rebin_dv(p, r.n, p.sm_lo, &v)) && rebin_in_rows(p, rebin_dv(p, r.n, p.sm_hi, &v));
+  r.col = p.raw + (size_t)(i - p.view0) * p.W * p.H;
+  return r;
+}
+
+__device__ __forceinline__ float rebin_view_angle(const RebinParams& p, int s, int ib) {
+  const int st = p.start[s];
+  const long long i = (long long)st + ib;
+  if (st < 0 || i < 1) return 0.f;
+  float lam = __fadd_rn(__fmul_rn((float)(i - 1), p.delta), p.BV);
+  while (lam > p.twopi) lam = __fsub_rn(lam, p.twopi);
+  return lam;
+}
+
+// one output sample of a valid row
+__device__ __forceinline__ float rebin_sample(const RebinParams& p, const RebinRow& r, int j) {
+  float v;
+  const float dv = rebin_dv(p, r.n, __ldg(p.sm + j), &v);
+  int idv = (int)floorf(dv);
+  idv = min(max(idv, 1), p.H - 1);  // already so for a valid row; keeps the loads in bounds regardless
+  const float t = __fsub_rn(dv, (float)idv);
+  const float* c = r.col + (size_t)j * p.H + (idv - 1);
+  const float d0 = __ldg(c), d1 = __ldg(c + 1);
+  const float temp = __fadd_rn(__fmul_rn(d0, __fsub_rn(1.0f, t)), __fmul_rn(d1, t));
+  const float cosv = __fdiv_rn(p.SD, __fsqrt_rn(__fadd_rn(p.SD2, __fmul_rn(v, v))));
+  return __fmul_rn(cosv, temp);
+}
+
+constexpr int kRowsPerCta = 8;  // one warp per output row
+
+// Reference (mex) layout: out[s][ib][j], views[s][ib].  One warp per row,
+// lanes over channels: coalesced stores; each sample loads two adjacent rows
+// of one detector column.
+__global__ void __launch_bounds__(256) k_rebin_mex(RebinParams p) {
+  const int lane = threadIdx.x & 31;
+  const int ib = blockIdx.x * kRowsPerCta + (threadIdx.x >> 5);
+  const int s = blockIdx.y;
+  if (ib >= p.T) return;
+  const RebinRow r = rebin_row(p, s, ib);
+  float* o = p.out + ((size_t)s * p.T + ib) * p.W;
+  if (r.ok) {
+    for (int j = lane; j < p.W; j += 32) o[j] = rebin_sample(p, r, j);
+  } else {
+    for (int j = lane; j < p.W; j += 32) o[j] = 0.f;
+  }
+  if (lane == 0) p.views[(size_t)s * p.T + ib] = rebin_view_angle(p, s, ib);
+}
+
+// Routine layout (after HelicalToFan_routine.m:44-45 permutes, the solver's
+// sinogram layout): out[ib][j][s], views[ib][s].  A CTA owns 32 slices of one
+// view; warps compute rows (lanes over 32 channels) into a shared tile, then
+// store it transposed with lanes over slices (128-byte rows).
+__global__ void __launch_bounds__(256) k_rebin_routine(RebinParams p) {
+  __shared__ float tile[32][33];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int ib = blockIdx.x;
+  const int s0 = blockIdx.y * 32;
+  RebinRow rows[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int s = s0 + warp * 4 + q;
+    if (s < p.SLN) {
+      rows[q] = rebin_row(p, s, ib);
+    } else {
+      rows[q].ok = false;
+      rows[q].col = nullptr;
+      rows[q].n = 0.f;
+    }
+  }
+  if (warp == 0 && s0 + lane < p.SLN)
+    p.views[(size_t)ib * p.SLN + s0 + lane] = rebin_view_angle(p, s0 + lane, ib);
+  const int ns = min(32, p.SLN - s0);
+  for (int j0 = 0; j0 < p.W; j0 += 32) {
+    const int j = j0 + lane;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      tile[warp * 4 + q][lane] = (rows[q].ok && j < p.W) ? rebin_sample(p, rows[q], j) : 0.f;
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int jj = j0 + warp * 4 + q;
+      if (jj < p.W && lane < ns) p.out[((size_t)ib * p.W + jj) * p.SLN + s0 + lane] = tile[lane][warp * 4 + q];
+    }
+    __syncthreads();
+  }
+}
+
+struct RebinHost {
+  RebinParams p;
+  std::vector<float> sm;
+  std::vector<int> start;
+  long long lo = 0, hi = -1;  // 1-based raw views the computed rows read (empty when hi < lo)
+};
+
+// Host constants exactly as HelicalToFan (HelicalToFanFunc_mex.cpp:160-164) and
+// HelicalToFanImpl (:66, :80-84) compute them, plus argument checks.
+int rebin_prepare(RebinHost& h, long long nViews, const float* zPos, int SLN, float SD, float SO,
+                  float BVAngle, int DetWidth, int DetHeight, float PerDetW, float PerDetH,
+                  int DefTimes, float DetCenterW, float SpiralPitchFactor) {
+  if (!zPos) return set_err(DDFAN_ERR_ARG, "HelicalToFan: null zPos");
+  if (SLN < 1 || DetWidth < 1 || DetHeight < 2 || DefTimes < 1 || nViews < 1 || SLN > 65535)
+    return set_err(DDFAN_ERR_ARG, "HelicalToFan: bad sizes (SLN=%d DetWidth=%d DetHeight=%d DefTimes=%d views=%lld)",
+                   SLN, DetWidth, DetHeight, DefTimes, nViews);
+  const float PerDetA = 2.0f * atanf(PerDetW / SD * 0.5f);
+  const float delta = 2.0 * M_PI / DefTimes;
+  const float DetCenterHreal = (DetHeight - 1.0) * 0.5 / PerDetH;
+  const float hh = SpiralPitchFactor * PerDetH * DetHeight * SO / SD;
+  const float deltaZ = hh / DefTimes;
+  if (!std::isfinite(deltaZ) || !(std::fabs(deltaZ) > 0.f) || !std::isfinite(SD) || !std::isfinite(PerDetH) ||
+      PerDetH == 0.f)
+    return set_err(DDFAN_ERR_ARG, "HelicalToFan: degenerate geometry (deltaZ=%g SD=%g PerDetH=%g)", deltaZ, SD,
+                   PerDetH);
+  h.sm.resize(DetWidth);
+  float lo = INFINITY, hi = -INFINITY;
+  for (int j = 1; j <= DetWidth; ++j) {
+    const float ang = (j - DetCenterW) * PerDetA;
+    const float SM = SO * cosf(ang);
+    h.sm[j - 1] = SM;
+    lo = std::min(lo, SM);
+    hi = std::max(hi, SM);
+  }
+  // the one-pair row test needs every SM_j finite and of one sign
+  if (!std::isfinite(lo) || !std::isfinite(hi) || !((lo > 0.f) || (hi < 0.f)))
+    return set_err(DDFAN_ERR_UNSUPPORTED, "HelicalToFan: channel fan angles reach 90 degrees (SO*cos in [%g, %g])",
+                   lo, hi);
+  h.start.resize(SLN);
+  h.lo = (long long)1 << 62;
+  h.hi = -1;
+  for (int s = 0; s < SLN; ++s) {
+    const float z = zPos[s];
+    const float q = floorf((z - hh * 0.5f) / deltaZ);
+    if (!std::isfinite(q) || std::fabs(q) > 1.0e9f)
+      return set_err(DDFAN_ERR_ARG, "HelicalToFan: zPos[%d] = %g is far outside the scan", s, z);
+    const int st = (int)q;
+    h.start[s] = st;
+    if (st < 0) continue;  // the reference leaves such a slice zero
+    const long long last = (long long)st + DefTimes - 1;
+    if (last > nViews)
+      return set_err(DDFAN_ERR_ARG, "HelicalToFan: slice %d (z = %g) needs raw view %lld, only %lld given", s, z, last,
+                     nViews);
+    if (last >= 1) {
+      h.lo = std::min(h.lo, std::max(1LL, (long long)st));
+      h.hi = std::max(h.hi, last);
+    }
+  }
+  if (h.hi < h.lo) h.lo = 1, h.hi = 0;
+  RebinParams& p = h.p;
+  p = RebinParams{};
+  p.SLN = SLN; p.T = DefTimes; p.W = DetWidth; p.H = DetHeight;
+  p.SD = SD; p.SD2 = SD * SD; p.PH = PerDetH; p.DCH = DetCenterHreal;
+  p.deltaZ = deltaZ; p.delta = delta; p.BV = BVAngle; p.twopi = (float)(2 * M_PI);
+  p.sm_lo = lo; p.sm_hi = hi;
+  return DDFAN_OK;
+}
+
+int rebin_launch(const RebinParams& p, int layout, cudaStream_t st) {
+  if (layout == 0) {
+    dim3 grid((p.T + kRowsPerCta - 1) / kRowsPerCta, p.SLN);
+    k_rebin_mex<<<grid, 256, 0, st>>>(p);
+  } else {
+    if (p.T > 0x7fffffff) return set_err(DDFAN_ERR_ARG, "HelicalToFan: DefTimes too large");
+    dim3 grid(p.T, (p.SLN + 31) / 32);
+    k_rebin_routine<<<grid, 256, 0, st>>>(p);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "HelicalToFan launch: %s", cudaGetErrorString(e));
+  return DDFAN_OK;
+}
+
+// small host->device uploads of the per-channel and per-slice tables into one buffer
+int rebin_tables(RebinHost& h, const float* zPos, void** buf, cudaStream_t st) {
+  const int W = h.p.W, SLN = h.p.SLN;
+  const size_t b_sm = ((sizeof(float) * W + 255) / 256) * 256;
+  const size_t b_z = ((sizeof(float) * SLN + 255) / 256) * 256;
+  const size_t bytes = b_sm + b_z + sizeof(int) * SLN;
+  int rc = dev_alloc(buf, bytes, st);
+  if (rc) return rc;
+  unsigned char* b = static_cast<unsigned char*>(*buf);
+  cudaError_t e = cudaMemcpyAsync(b, h.sm.data(), sizeof(float) * W, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(b + b_sm, zPos, sizeof(float) * SLN, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b + b_sm + b_z, h.start.data(), sizeof(int) * SLN, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(DDFAN_ERR_CUDA, "HelicalToFan table upload: %s", cudaGetErrorString(e));
+  }
+  h.p.sm = reinterpret_cast<const float*>(b);
+  h.p.zpos = reinterpret_cast<const float*>(b + b_sm);
+  h.p.start = reinterpret_cast<const int*>(b + b_sm + b_z);
+  return DDFAN_OK;
+}
+
+}  // namespace
+}  // namespace ddfan
+
+using namespace ddfan;
+
+extern "C" DDFAN_API int ddfan_helical_to_fan_dev(const float* d_proj, long long nViews, const float* zPos, int SLN,
+                                                  float SD, float SO, float BVAngle, int DetWidth, int DetHeight,
+                                                  float PerDetW, float PerDetH, int DefTimes, float DetCenterW,
+                                                  float SpiralPitchFactor, int layout, float* d_Proj,
+                                                  float* d_Views, void* stream) {
+  if (!d_proj || !d_Proj || !d_Views) return set_err(DDFAN_ERR_ARG, "helical_to_fan_dev: null argument");
+  if (layout != 0 && layout != 1) return set_err(DDFAN_ERR_ARG, "helical_to_fan_dev: layout %d", layout);
+  RebinHost h;
+  int rc = rebin_prepare(h, nViews, zPos, SLN, SD, SO, BVAngle, DetWidth, DetHeight, PerDetW, PerDetH, DefTimes,
+                         DetCenterW, SpiralPitchFactor);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  void* tables = nullptr;
+  if ((rc = rebin_tables(h, zPos, &tables, st))) return rc;
+  h.p.raw = d_proj;
+  h.p.view0 = 1;
+  h.p.out = d_Proj;
+  h.p.views = d_Views;
+  rc = rebin_launch(h.p, layout, st);
+  dev_free(tables, st);
+  return rc;
+}
+
+extern "C" DDFAN_API int ddfan_HelicalToFan(float* Proj, float* Views, const float* proj, long long nViews,
+                                            const float* zPos, int SLN, float SD, float SO, float BVAngle,
+                                            int DetWidth, int DetHeight, float PerDetW, float PerDetH,
+                                            int DefTimes, float DetCenterW, float SpiralPitchFactor) {
+  if (!Proj || !Views || !proj) return set_err(DDFAN_ERR_ARG, "HelicalToFan: null argument");
+  RebinHost h;
+  int rc = rebin_prepare(h, nViews, zPos, SLN, SD, SO, BVAngle, DetWidth, DetHeight, PerDetW, PerDetH, DefTimes,
+                         DetCenterW, SpiralPitchFactor);
+  if (rc) return rc;
+  cudaStream_t st = nullptr;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(DDFAN_ERR_CUDA, "HelicalToFan: cudaStreamCreate failed");
+  }
+  const size_t view_elems = (size_t)DetWidth * DetHeight;
+  const size_t nraw = h.hi >= h.lo ? (size_t)(h.hi - h.lo + 1) : 0;
+  const size_t out_elems = (size_t)SLN * DefTimes * DetWidth;
+  void *d_raw = nullptr, *d_out = nullptr, *d_views = nullptr, *tables = nullptr;
+  rc = dev_alloc(&d_raw, std::max<size_t>(1, nraw) * view_elems * sizeof(float), st);
+  if (!rc) rc = dev_alloc(&d_out, out_elems * sizeof(float), st);
+  if (!rc) rc = dev_alloc(&d_views, (size_t)SLN * DefTimes * sizeof(float), st);
+  if (!rc) rc = rebin_tables(h, zPos, &tables, st);
+  if (!rc && nraw) {
+    // only the raw views some computed row reads travel to the device
+    cudaError_t e = cudaMemcpyAsync(d_raw, proj + (size_t)(h.lo - 1) * view_elems, nraw * view_elems * sizeof(float),
+                                    cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      rc = set_err(DDFAN_ERR_CUDA, "HelicalToFan: raw upload: %s", cudaGetErrorString(e));
+    }
+  }
+  if (!rc) {
+    h.p.raw = static_cast<const float*>(d_raw);
+    h.p.view0 = nraw ? h.lo : 1;
+    h.p.out = static_cast<float*>(d_out);
+    h.p.views = static_cast<float*>(d_views);
+    rc = rebin_launch(h.p, 0, st);
+  }
+  if (!rc) {
+    cudaError_t e = cudaMemcpyAsync(Proj, d_out, out_elems * sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(Views, d_views, (size_t)SLN * DefTimes * sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      rc = set_err(DDFAN_ERR_CUDA, "HelicalToFan: %s", cudaGetErrorString(e));
+    }
+  }
+  dev_free(tables, st);
+  dev_free(d_views, st);
+  dev_free(d_out, st);
+  dev_free(d_raw, st);
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  return rc;
+}

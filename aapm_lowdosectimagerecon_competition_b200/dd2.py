@@ -16,6 +16,11 @@ Reference entry points mirrored (paths relative to the reference project root):
   MultiSlicesBackGPU   AAPM_script/MultiSlicesBackGPU.cu:409-436
   DD2MutiSlices        AAPM_script/DD2MutiSlices.m:47-117
   OSSART_AAPM          AAPM_script/OSSART_AAPM.m:33-118
+  HelicalToFanFunc_mex AAPM_script/HelicalToFanFunc_mex.cpp:186-249 (body :41-185)
+  HelicalToFan_routine AAPM_script/HelicalToFan_routine.m:1-45
+
+Raw helical data: MATLAB single(DetHeight, DetWidth, TotalViews) <-> numpy
+float32 (TotalViews, DetWidth, DetHeight).
 """
 import ctypes
 
@@ -174,3 +179,51 @@ def OSSART_AAPM(Proj, Views, initImg, conf, numOfIter, numOfOS=1, mask=None, use
          int(useFISTA), int(nonneg), _mode(sat, SAT_MODES, "sat mode"),
          _mode(back, BACK_MODES, "back mode"), _ptr(out))
     return out
+
+
+def HelicalToFanFunc_mex(proj, zPos, SLN, SD, SO, BVAngle, DetWidth, DetHeight, PerDetW, PerDetH,
+                         DefTimes, DetCenterW, SpiralPitchFactor):
+    """The mex AAPM_script/HelicalToFanFunc_mex.cpp:186-249 on the GPU.
+
+    proj (TotalViews, DetWidth, DetHeight); returns the mex's layouts
+    Proj (SLN, DefTimes, DetWidth) and Views (SLN, DefTimes), bit-identical
+    to the reference's CPU result."""
+    proj = _f32(proj)
+    nViews = int(proj.shape[0])
+    if proj.size != nViews * int(DetWidth) * int(DetHeight):
+        raise ValueError("proj has %d values, expected TotalViews x DetWidth x DetHeight" % proj.size)
+    z = _f32(zPos).reshape(-1)
+    SLN = int(SLN)
+    if z.size < SLN:
+        raise ValueError("zPos has %d entries, SLN = %d" % (z.size, SLN))
+    P = np.empty((SLN, int(DefTimes), int(DetWidth)), np.float32)
+    V = np.empty((SLN, int(DefTimes)), np.float32)
+    call("ddfan_HelicalToFan", _ptr(P), _ptr(V), _ptr(proj), nViews, _ptr(z), SLN, SD, SO, BVAngle,
+         int(DetWidth), int(DetHeight), PerDetW, PerDetH, int(DefTimes), DetCenterW, SpiralPitchFactor)
+    return P, V
+
+
+def rebin_params(cfg):
+    """The scan constants AAPM_script/HelicalToFan_routine.m:20-33 reads from
+    the projection header cfg (nested dict or object; angle in degrees)."""
+    return dict(SD=np.float32(_get(cfg, "ConstantRadialDistance")),
+                SO=np.float32(_get(cfg, "DetectorFocalCenterRadialDistance")),
+                BVAngle=np.float32(_get(cfg, "DetectorFocalCenterAngularPosition") / 180.0 * np.pi),
+                DetWidth=int(_get(cfg, "NumberofDetectorColumns")),
+                DetHeight=int(_get(cfg, "NumberofDetectorRows")),
+                PerDetW=np.float32(_get(cfg, "DetectorElementTransverseSpacing")),
+                PerDetH=np.float32(_get(cfg, "DetectorElementAxialSpacing")),
+                DefTimes=int(_get(cfg, "NumberofSourceAngularSteps")),
+                DetCenterW=np.float32(_get(cfg, "DetectorCentralElement", "X")),
+                SpiralPitchFactor=np.float32(_get(cfg, "SpiralPitchFactor")))
+
+
+def HelicalToFan_routine(proj, cfg, zPos):
+    """AAPM_script/HelicalToFan_routine.m:1-45: rebin and permute.
+
+    Returns Proj (DefTimes, DetWidth, SLN) and Views (DefTimes, SLN) -- the
+    MATLAB (SLN, DetWidth, DefTimes) and (SLN, DefTimes) arrays, i.e. the
+    layouts OSSART_AAPM takes."""
+    z = _f32(zPos).reshape(-1)
+    P, V = HelicalToFanFunc_mex(proj, z, z.size, **rebin_params(cfg))
+    return np.ascontiguousarray(P.transpose(1, 2, 0)), np.ascontiguousarray(V.T)

@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--kernels", action="store_true",
                     help="time only one subset's projector kernels (small case for ncu captures)")
-    ap.add_argument("--config", default="c3", choices=["c3", "c4", "c5"],
+    ap.add_argument("--config", default="c3", choices=["c3", "c4", "c5", "rebin"],
                     help="c3: the OS-SART contract line; c4: batched uneven reconstructions; "
                          "c5: Poisson-arrival serving")
     ap.add_argument("--instances", type=int, default=32)
@@ -125,6 +125,234 @@ def run_c5(args):
             "throughput_vs_serial_device_fp32": served["samples_per_s"] / pb["samples_per_s"],
             "budget_gb": 150, "data": "synthetic"}
     print(json.dumps(line), flush=True)
+
+
+REBIN_METRIC = "helical-to-fan rebinned slices/s (736x64 detector, 2304 views/rotation, 512 slices)"
+REBIN_UNIT = "slices/s"
+
+
+def rebin_workload(rotations=10, SLN=512):
+    """Siemens-like helical scan: 736 channels x 64 rows, 2304 views per
+    rotation, pitch 0.8, `rotations` turns of raw views; slice positions
+    linspace(h, deltaZ * TotalView - h, SLN) as AAPM_script/reconscript.m:22."""
+    f = np.float32
+    p = dict(SD=f(1085.6), SO=f(595.0), BVAngle=f(0.0), DetWidth=736, DetHeight=64, PerDetW=f(1.2858),
+             PerDetH=f(1.0947), DefTimes=2304, DetCenterW=f(369.625), SpiralPitchFactor=f(0.8))
+    TV = rotations * p["DefTimes"]
+    h = p["SpiralPitchFactor"] * p["PerDetH"] * f(p["DetHeight"]) * p["SO"] / p["SD"]
+    dZ = h / f(p["DefTimes"])
+    z = np.linspace(float(h), float(dZ) * TV - float(h), SLN).astype(np.float32)
+    return p, TV, z
+
+
+def rebin_config(p, TV, z):
+    return {"workload": "helical-to-fan rebinning: %d raw views of %dx%d, %d views/rotation, %d slices"
+                        % (TV, p["DetWidth"], p["DetHeight"], p["DefTimes"], z.size),
+            "raw_views": TV, "DetWidth": p["DetWidth"], "DetHeight": p["DetHeight"],
+            "DefTimes": p["DefTimes"], "SLN": int(z.size), "pitch": float(p["SpiralPitchFactor"]),
+            "l2": "inputs larger than L2 (raw views %.1f GB)" % (TV * p["DetWidth"] * p["DetHeight"] * 4 / 1e9)}
+
+
+def rebin_cpu_timing(proj, z, p, slices):
+    """Seconds per slice of the reference's own CPU HelicalToFan
+    (oracle/_ref/libref_rebin.so, kind "reference") on the first `slices`
+    slices, else of the numpy restatement (kind "port")."""
+    ref = os.path.join(ROOT, "oracle", "_ref", "libref_rebin.so")
+    zz = np.ascontiguousarray(z[:slices])
+    if os.path.exists(ref):
+        sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+        import make_rebin_fixtures as M
+        lib = M.load_reference()
+        t0 = time.perf_counter()
+        M.run_reference(lib, proj, zz, p["SD"], p["SO"], p["BVAngle"], p["DetWidth"], p["DetHeight"],
+                        p["PerDetW"], p["PerDetH"], p["DefTimes"], p["DetCenterW"], p["SpiralPitchFactor"])
+        return (time.perf_counter() - t0) / slices, "reference", os.cpu_count() or 1
+    from oracle import np_oracle as N
+    t0 = time.perf_counter()
+    N.helical_to_fan(proj, zz, **p)
+    return (time.perf_counter() - t0) / slices, "port", 1
+
+
+def rebin_last_view(p, z):
+    """Largest 1-based raw view the slices at z read (HelicalToFanFunc_mex.cpp:66,73)."""
+    f = np.float32
+    h = p["SpiralPitchFactor"] * p["PerDetH"] * f(p["DetHeight"]) * p["SO"] / p["SD"]
+    dZ = h / f(p["DefTimes"])
+    starts = np.floor((np.asarray(z, np.float32) - h * f(0.5)) / dZ).astype(np.int64)
+    return int(starts.max()) + p["DefTimes"] - 1
+
+
+def _rebin_host_raw(p, TV, seed=11):
+    rng = np.random.default_rng(seed)
+    return rng.random((TV, p["DetWidth"], p["DetHeight"]), dtype=np.float32)
+
+
+def run_rebin_reference(args):
+    """--impl reference --config rebin: the reference's CPU rebinning on a
+    bounded sample of slices per step (rank 0 only)."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    p, TV, z = rebin_workload()
+    sample = 32
+    # only the raw views the sampled slices read are generated
+    proj = _rebin_host_raw(p, min(TV, rebin_last_view(p, z[:sample])))
+    rebin_cpu_timing(proj, z, p, 2)
+    per = []
+    kind, cores = "reference", 1
+    for _ in range(args.steps):
+        sec, kind, cores = rebin_cpu_timing(proj, z, p, sample)
+        per.append(sec)
+    sec = statistics.mean(per)
+    v = 1.0 / sec
+    line = {"impl": "reference", "metric": REBIN_METRIC, "value": v, "unit": REBIN_UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * z.size * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": rebin_config(p, TV, z),
+            "cpu_baseline": {"value": v, "unit": REBIN_UNIT, "cores": cores, "kind": kind,
+                             "sample": "first %d of %d slices per step; the reference starts one thread per "
+                                       "core but every thread's slice range begins at 0 "
+                                       "(HelicalToFanFunc_mex.cpp:165-181), so the last thread rebins all "
+                                       "of them" % (sample, z.size)},
+            "e2e": {"value": v, "unit": REBIN_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_rebin(args):
+    """--config rebin: GPU rebinning of the whole scan per step."""
+    import ctypes
+    import torch
+    import torch.distributed as dist
+    from aapm_lowdosectimagerecon_competition_b200 import dd2
+    from aapm_lowdosectimagerecon_competition_b200._lib import call
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    p, TV, z = rebin_workload()
+    SLN, T, W, H = z.size, p["DefTimes"], p["DetWidth"], p["DetHeight"]
+    g = torch.Generator(device=dev)
+    g.manual_seed(11 + rank)
+    d_raw = torch.rand((TV, W, H), generator=g, device=dev, dtype=torch.float32)
+    d_out = torch.empty((T, W, SLN), device=dev, dtype=torch.float32)
+    d_views = torch.empty((T, SLN), device=dev, dtype=torch.float32)
+    stream = torch.cuda.current_stream(dev)
+    zp = z.ctypes.data_as(ctypes.c_void_p)
+    V = lambda t: ctypes.c_void_p(t.data_ptr())
+
+    def launch(layout, out=d_out, views=d_views):
+        call("ddfan_helical_to_fan_dev", V(d_raw), TV, zp, SLN, p["SD"], p["SO"], p["BVAngle"], W, H,
+             p["PerDetW"], p["PerDetH"], T, p["DetCenterW"], p["SpiralPitchFactor"], layout, V(out), V(views),
+             ctypes.c_void_p(stream.cuda_stream))
+
+    for _ in range(max(args.warmup, 3)):
+        launch(1)
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        launch(1)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    ms_per_step = ms_max / args.steps
+    value = world * SLN * args.steps / (ms_max / 1e3)
+
+    # mex layout (reference output order), for the roofline comparison
+    d_out0 = torch.empty((SLN, T, W), device=dev, dtype=torch.float32)
+    d_views0 = torch.empty((SLN, T), device=dev, dtype=torch.float32)
+    launch(0, d_out0, d_views0)
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e2.record(stream)
+    for _ in range(args.steps):
+        launch(0, d_out0, d_views0)
+    e3.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_mex = e2.elapsed_time(e3) / args.steps
+    same = bool(torch.equal(d_out0.permute(1, 2, 0), d_out) and torch.equal(d_views0.t(), d_views))
+    del d_out0, d_views0
+
+    # algorithmic bytes: every raw view some slice reads (all of them here) + the outputs
+    f = np.float32
+    h = p["SpiralPitchFactor"] * p["PerDetH"] * f(H) * p["SO"] / p["SD"]
+    dZ = h / f(T)
+    starts = np.floor((z - h * f(0.5)) / dZ).astype(np.int64)
+    lo, hi = max(1, int(starts.min())), int(starts.max()) + T - 1
+    raw_bytes = (hi - lo + 1) * W * H * 4
+    alg = raw_bytes + SLN * T * W * 4 + SLN * T * 4
+    peak, peak_kind = peaks()
+    achieved = alg / (ms_per_step / 1e3) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "k_rebin_routine.md")) as fh:
+            for ln in fh:
+                if ln.startswith("traffic_bytes_per_launch:"):
+                    traffic = float(ln.split(":", 1)[1])
+    except OSError:
+        pass
+    roofline = {"bound": "hbm", "kernel": "k_rebin_routine", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic, "algorithmic_bytes": alg,
+                "launch_ms": ms_per_step, "mex_layout_launch_ms": ms_mex, "layouts_agree": same,
+                "note": "algorithmic bytes = raw views read once + rebinned sinogram + view angles"}
+    line = {"metric": REBIN_METRIC, "value": value, "unit": REBIN_UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": rebin_config(p, TV, z),
+            "gpu_launches": args.steps, "clocks": clk, "roofline": roofline}
+
+    if not args.no_e2e or (rank == 0 and world == 1 and not args.no_cpu):
+        proj_h = d_raw.cpu().numpy()
+    if not args.no_e2e:
+        t_e2e = []
+        for rep in range(2):
+            torch.cuda.synchronize(dev)
+            if world > 1:
+                dist.barrier()
+            t0 = time.perf_counter()
+            P, Vw = dd2.HelicalToFanFunc_mex(proj_h, z, SLN, **p)
+            t_e2e.append(time.perf_counter() - t0)
+        te = min(t_e2e[1:] or t_e2e)
+        tt = torch.tensor([te], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        te = float(tt.item())
+        line["e2e"] = {"value": world * SLN / te, "unit": REBIN_UNIT, "h2d_bytes_per_step": int(raw_bytes + SLN * 4),
+                       "d2h_bytes_per_step": int(SLN * T * W * 4 + SLN * T * 4),
+                       "step": "one ddfan_HelicalToFan call from pageable host arrays (mex layouts): "
+                               "upload of the raw views the slices read, rebinning, download",
+                       "seconds_per_call": te}
+        del P, Vw
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sample = 32
+        sec, kind, cores = rebin_cpu_timing(proj_h, z, p, sample)
+        line["cpu_baseline"] = {"value": 1.0 / sec, "unit": REBIN_UNIT, "cores": cores, "kind": kind,
+                                "sample": "first %d of %d slices; the reference's thread split gives every "
+                                          "thread a range starting at slice 0, so the last thread rebins all"
+                                          % (sample, SLN)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_kernels(args):
@@ -479,7 +707,12 @@ def plain_fp32_iteration(s, geom, y, mask):
 def main():
     args = parse()
     if args.impl == "reference":
-        run_reference(args)
+        if args.config == "rebin":
+            run_rebin_reference(args)
+        else:
+            run_reference(args)
+    elif args.config == "rebin":
+        run_rebin(args)
     elif args.kernels:
         run_kernels(args)
     elif args.config == "c4":

@@ -197,6 +197,32 @@ DDFAN_API int ddfan_OSSART_AAPM(float x0, float y0, int DNU, const float* xds, c
                                 int numOfIter, int numOfOS, int useFISTA, int nonneg,
                                 int sat_mode, int back_mode, float* reconImg);
 
+/* ---- Helical-to-fan single-slice rebinning ----
+ * Replaces the CPU mex HelicalToFan (AAPM_script/HelicalToFanFunc_mex.cpp:142-185,
+ * per-slice body HelicalToFanImpl :41-139; MATLAB entry HelicalToFanFunc_mex
+ * called from HelicalToFan_routine.m:39-42) with the same argument meaning and a
+ * bit-identical result.  proj: raw helical views [nViews][DetWidth][DetHeight]
+ * (MATLAB (Height, Channel, View)); zPos[SLN] target slice positions; outputs in
+ * the mex's layouts Proj[SLN][DefTimes][DetWidth] and Views[SLN][DefTimes].
+ * nViews is the number of raw views (the mex reads it from the array; a slice
+ * that needs a view beyond it is DDFAN_ERR_ARG, where the reference reads past
+ * its buffer).  A slice with floor((z - h/2) / deltaZ) < 0 is all zero, as in
+ * the reference.  Host pointers; runs on the current device. */
+DDFAN_API int ddfan_HelicalToFan(float* Proj, float* Views, const float* proj, long long nViews,
+                                 const float* zPos, int SLN, float SD, float SO, float BVAngle,
+                                 int DetWidth, int DetHeight, float PerDetW, float PerDetH,
+                                 int DefTimes, float DetCenterW, float SpiralPitchFactor);
+/* Device-resident variant: d_proj[nViews][DetWidth][DetHeight] on the device,
+ * zPos on the host.  layout 0 writes the mex layouts above; layout 1 writes the
+ * layouts HelicalToFan_routine.m:44-45 returns after its permutes,
+ * d_Proj[DefTimes][DetWidth][SLN] and d_Views[DefTimes][SLN] (the sinogram
+ * layout ddfan_ossart_set_sinogram takes).  Stream-ordered; no host sync. */
+DDFAN_API int ddfan_helical_to_fan_dev(const float* d_proj, long long nViews, const float* zPos,
+                                       int SLN, float SD, float SO, float BVAngle, int DetWidth,
+                                       int DetHeight, float PerDetW, float PerDetH, int DefTimes,
+                                       float DetCenterW, float SpiralPitchFactor, int layout,
+                                       float* d_Proj, float* d_Views, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

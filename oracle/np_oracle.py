@@ -9,10 +9,20 @@ Reference formulas followed (paths relative to the reference project root):
   boundaries         AAPM_script/utilities.cuh:268-287
   system_matrix      AAPM_script/MultiSlicesProjGPU.cu:100-200 (per-ray footprint per line)
   back_ref           AAPM_script/MultiSlicesBackGPU.cu:115-184, host :187-242
+  helical_to_fan     AAPM_script/HelicalToFanFunc_mex.cpp:41-185
 """
+import ctypes
+import ctypes.util
+
 import numpy as np
 
 TWOPI = 6.283185307179586
+
+_libm = ctypes.CDLL(ctypes.util.find_library("m") or "libm.so.6")
+_libm.cosf.restype = ctypes.c_float
+_libm.cosf.argtypes = [ctypes.c_float]
+_libm.atanf.restype = ctypes.c_float
+_libm.atanf.argtypes = [ctypes.c_float]
 
 
 def fan_geometry(sid, sdd, DNU, detCellWidth, detCntIdx):
@@ -109,6 +119,70 @@ def system_matrix(x0, y0, xds, yds, imgXCenter, imgYCenter, angles, XN, YN, dx, 
         m = np.asarray(mask, np.uint8).reshape(-1)[: XN * YN].astype(np.float64)
         A = A * m[None, :]
     return A
+
+
+def helical_to_fan(proj, zPos, SD, SO, BVAngle, DetWidth, DetHeight, PerDetW, PerDetH, DefTimes,
+                   DetCenterW, SpiralPitchFactor):
+    """Single-slice helical-to-fan rebinning in the reference's float32
+    arithmetic (AAPM_script/HelicalToFanFunc_mex.cpp:41-185).
+
+    proj: raw helical data [TotalViews][DetWidth][DetHeight] (MATLAB
+    (Height, Channel, View)).  Returns Proj [DefTimes][DetWidth][SLN] and
+    Views [DefTimes][SLN] -- the layouts HelicalToFan_routine.m:44-45 leaves
+    after its permutes.  cosf/atanf come from the C library, the functions
+    the reference calls, so the result is bit-identical to it on one host."""
+    f = np.float32
+    proj = np.asarray(proj, np.float32)
+    zPos = np.asarray(zPos, np.float32)
+    SLN = zPos.size
+    SD, SO, BVAngle, PerDetW, PerDetH, DetCenterW, SpiralPitchFactor = (
+        f(SD), f(SO), f(BVAngle), f(PerDetW), f(PerDetH), f(DetCenterW), f(SpiralPitchFactor))
+    PerDetA = f(2.0) * f(_libm.atanf(float(PerDetW / SD * f(0.5))))      # :160
+    delta = f(2.0 * np.pi / DefTimes)                                      # :161
+    DetCenterHreal = f((DetHeight - 1.0) * 0.5 / float(PerDetH))           # :162 (divides by PerDetH)
+    h = SpiralPitchFactor * PerDetH * f(DetHeight) * SO / SD               # :163
+    deltaZ = h / f(DefTimes)                                               # :164
+    twopi = f(2.0 * np.pi)
+    Proj = np.zeros((DefTimes, DetWidth, SLN), np.float32)
+    Views = np.zeros((DefTimes, SLN), np.float32)
+    j = np.arange(1, DetWidth + 1)
+    ang = (j.astype(np.float32) - DetCenterW) * PerDetA
+    SM = SO * np.array([_libm.cosf(float(a)) for a in ang], np.float32)
+    for iii in range(SLN):
+        z = zPos[iii]
+        start = int(np.floor((z - h * f(0.5)) / deltaZ))
+        PData = np.zeros((DefTimes, DetWidth), np.float32)
+        mark = np.zeros((DefTimes, DetWidth), np.int32)
+        angles = np.zeros(DefTimes, np.float32)
+        # the reference's loop index is size_t: `i >= start` never holds for
+        # start < 0 (the slice stays zero), and i starts at 1 (:73-76)
+        first = start + DefTimes if start < 0 else max(1, start)
+        for i in range(first, start + DefTimes):
+            data = proj[i - 1]                                             # [DetWidth][DetHeight]
+            zz = f(i - 1) * deltaZ
+            lam = f(i - 1) * delta + BVAngle
+            while lam > twopi:                                             # AAPM::mod (:28-34)
+                lam = lam - twopi
+            ib = i - start                                                 # ibeta - 1
+            angles[ib] = lam
+            tanAngV = (z - zz) / SM
+            v = SD * tanAngV
+            dv = (DetCenterHreal + v) / PerDetH + f(1.0)
+            idv = np.floor(dv).astype(np.int64)
+            t = dv - idv.astype(np.float32)
+            cosAngV = SD / np.sqrt(SD * SD + v * v)
+            ok = (idv >= 1) & (idv <= DetHeight - 1)
+            ii = np.clip(idv, 1, DetHeight - 1)
+            d0 = data[j - 1, ii - 1]
+            d1 = data[j - 1, ii]
+            temp = np.where(ok, d0 * (f(1.0) - t) + d1 * t, f(0.0)).astype(np.float32)
+            PData[ib] = cosAngV * temp
+            mark[ib] = ok
+        bad = (mark == 0).any(axis=1)                                      # :113-123
+        PData[bad] = 0
+        Proj[:, :, iii] = PData
+        Views[:, iii] = angles
+    return Proj, Views
 
 
 def back_ref(x0, y0, xds, yds, detCntIdx, imgXCenter, imgYCenter, angles, XN, YN, dx, prj,
