@@ -315,7 +315,7 @@ template <int M>
 static int sat_dispatch(const SatSrc& s, float4* out0, int nl0, float4* out1, int nl1, int N0, int N1,
                         int Nw0, int Nw1, int ZB, int ntab, cudaStream_t st) {
   const int Nw = std::max(Nw0, Nw1);
-  dim3 grid(std::max(nl0, nl1), (ZB + 7) / 8, ntab);
+  dim3 grid(std::max(nl0, nl1), (s.zb1 - s.zb0 + 7) / 8, ntab);
   // 512 threads = 8 z lanes x 64 chunks of C cells
   if (Nw <= 64 * 2) k_sat<M, 2><<<grid, 512, 0, st>>>(s, out0, nl0, nl1, out1, N0, N1, Nw0, Nw1, ZB);
   else if (Nw <= 64 * 4) k_sat<M, 4><<<grid, 512, 0, st>>>(s, out0, nl0, nl1, out1, N0, N1, Nw0, Nw1, ZB);
@@ -338,19 +338,40 @@ static int sat_launch(int mode, const SatSrc& s, float4* out0, int nl0, float4* 
 
 // Both image tables (rows -> satx, columns -> saty) in one launch; the mask
 // multiply of AAPM_script/MultiSlicesProjGPU.cu:202-209 happens on load.
-int launch_sat_image(const Plan& p, const float* d_vol, cudaStream_t st) {
+// z-blocks holding slices [zlo, zhi)
+static void zblock_range(const Plan& p, int zlo, int zhi, int* zb0, int* zb1) {
+  if (zhi < 0 || zhi > p.Z) zhi = p.Z;
+  zlo = std::max(0, std::min(zlo, zhi));
+  *zb0 = zlo / 4;
+  *zb1 = std::max(*zb0, (zhi + 3) / 4);
+}
+
+// z-tiles (ZL z-blocks each) holding slices [zlo, zhi)
+static void ztile_range(const Plan& p, int zlo, int zhi, int* zt0, int* nzt) {
+  int zb0, zb1;
+  zblock_range(p, zlo, zhi, &zb0, &zb1);
+  *zt0 = zb0 / p.ZL;
+  *nzt = zb1 > zb0 ? (zb1 + p.ZL - 1) / p.ZL - *zt0 : 0;
+}
+
+int launch_sat_image(const Plan& p, const float* d_vol, cudaStream_t st, int zlo, int zhi) {
   SatSrc s{};
   s.kind = 0; s.a = d_vol; s.mask = p.has_mask ? p.d_mask : nullptr;
   s.XN = p.XN; s.YN = p.YN; s.U = p.U; s.Z = p.Z; s.ZLt = p.ZL;
+  zblock_range(p, zlo, zhi, &s.zb0, &s.zb1);
+  if (s.zb1 <= s.zb0) return DDFAN_OK;
   ProfScope ps(KIND_SAT_IMAGE, st);
   return sat_launch(p.mode, s, p.d_satx, p.YN, p.d_saty, p.XN, p.XN, p.YN, p.XN, p.YN, p.ZB, 2, st);
 }
 
 int launch_sat_sino(const Plan& p, const float* d_prj, int PN, const float* wgt, float wscale,
-                    const float* y, const int* yview, const float* rowsum, cudaStream_t st) {
+                    const float* y, const int* yview, const float* rowsum, cudaStream_t st, int zlo,
+                    int zhi) {
   SatSrc s{};
   s.kind = 2; s.a = d_prj; s.wgt = wgt; s.wscale = wscale; s.y = y; s.yview = yview;
   s.rowsum = rowsum; s.XN = p.XN; s.YN = p.YN; s.U = p.U; s.Z = p.Z; s.ZLt = p.ZL;
+  zblock_range(p, zlo, zhi, &s.zb0, &s.zb1);
+  if (s.zb1 <= s.zb0) return DDFAN_OK;
   ProfScope ps(KIND_SAT_SINO, st);
   return sat_launch(p.mode, s, p.d_satq, PN, nullptr, 0, p.U, 0, p.U + 1, 0, p.ZB, 1, st);
 }
@@ -366,20 +387,20 @@ int launch_view_order(const ViewGeom* vg, int PN, int* order, int* counts, cudaS
 template <int ZL> struct FwdCG { static constexpr int v = ZL >= 4 ? 4 : (ZL == 2 ? 2 : 1); };
 
 template <int M, int ZL>
-static void fwd_go(const FwdArgs& a, cudaStream_t st) {
+static void fwd_go(const FwdArgs& a, int nzt, cudaStream_t st) {
   constexpr int CG = FwdCG<ZL>::v;
   using T = FwdTile<ZL, CG>;
-  dim3 grid((a.U + T::CW - 1) / T::CW, a.PN, (a.ZB + ZL - 1) / ZL);
+  dim3 grid((a.U + T::CW - 1) / T::CW, a.PN, nzt);
   k_fwd<M, ZL, CG><<<grid, T::NT, 0, st>>>(a);
 }
 
 template <int M>
-static void fwd_zl(int ZL, const FwdArgs& a, cudaStream_t st) {
+static void fwd_zl(int ZL, const FwdArgs& a, int nzt, cudaStream_t st) {
   switch (ZL) {
-    case 8: fwd_go<M, 8>(a, st); break;
-    case 4: fwd_go<M, 4>(a, st); break;
-    case 2: fwd_go<M, 2>(a, st); break;
-    default: fwd_go<M, 1>(a, st); break;
+    case 8: fwd_go<M, 8>(a, nzt, st); break;
+    case 4: fwd_go<M, 4>(a, nzt, st); break;
+    case 2: fwd_go<M, 2>(a, nzt, st); break;
+    default: fwd_go<M, 1>(a, nzt, st); break;
   }
 }
 
@@ -390,49 +411,52 @@ int launch_fwd(const Plan& p, const ViewGeom* vg, const double2* fc, const float
   a.satx = p.d_satx; a.saty = p.d_saty; a.vg = vg; a.fc = fc; a.cvd = cvd; a.order = order;
   a.out = d_prj; a.PN = PN; a.U = p.U; a.Z = p.Z; a.ZB = p.ZB; a.XN = p.XN; a.YN = p.YN;
   a.dx = p.dx; a.zlo = zlo; a.zhi = zhi;
+  int nzt = 0;
+  ztile_range(p, zlo, zhi, &a.zt0, &nzt);
+  if (nzt == 0) return DDFAN_OK;
   ProfScope ps(KIND_FWD, st);
   switch (p.mode) {
-    case SAT_FP32: fwd_zl<SAT_FP32>(p.ZL, a, st); break;
-    case SAT_HILO: fwd_zl<SAT_HILO>(p.ZL, a, st); break;
-    default: fwd_zl<SAT_FP64>(p.ZL, a, st); break;
+    case SAT_FP32: fwd_zl<SAT_FP32>(p.ZL, a, nzt, st); break;
+    case SAT_HILO: fwd_zl<SAT_HILO>(p.ZL, a, nzt, st); break;
+    default: fwd_zl<SAT_FP64>(p.ZL, a, nzt, st); break;
   }
   return check_launch("k_fwd");
 }
 
 template <int M, int ZL>
-static void ref_go(const RefArgs& a, cudaStream_t st) {
+static void ref_go(const RefArgs& a, int nzt, cudaStream_t st) {
   using T = BackTile<ZL>;
   const int tiles = ((a.YN + T::LT - 1) / T::LT) * ((a.XN + T::KT - 1) / T::KT);
-  dim3 grid(tiles, 1, (a.ZB + ZL - 1) / ZL);
+  dim3 grid(tiles, 1, nzt);
   k_back_ref<M, ZL><<<grid, T::NT, 0, st>>>(a);
 }
 
 template <int M, int ZL, bool XM>
-static void adj_go(const AdjArgs& a, cudaStream_t st) {
+static void adj_go(const AdjArgs& a, int nzt, cudaStream_t st) {
   using T = BackTile<ZL>;
   const int nl = XM ? a.XN : a.YN, N = XM ? a.YN : a.XN;
   const int tiles = ((nl + T::LT - 1) / T::LT) * ((N + T::KT - 1) / T::KT);
-  dim3 grid(tiles, 1, (a.ZB + ZL - 1) / ZL);
+  dim3 grid(tiles, 1, nzt);
   k_back_adj<M, ZL, XM><<<grid, T::NT, 0, st>>>(a);
 }
 
 template <int M>
-static void ref_zl(int ZL, const RefArgs& a, cudaStream_t st) {
+static void ref_zl(int ZL, const RefArgs& a, int nzt, cudaStream_t st) {
   switch (ZL) {
-    case 8: ref_go<M, 8>(a, st); break;
-    case 4: ref_go<M, 4>(a, st); break;
-    case 2: ref_go<M, 2>(a, st); break;
-    default: ref_go<M, 1>(a, st); break;
+    case 8: ref_go<M, 8>(a, nzt, st); break;
+    case 4: ref_go<M, 4>(a, nzt, st); break;
+    case 2: ref_go<M, 2>(a, nzt, st); break;
+    default: ref_go<M, 1>(a, nzt, st); break;
   }
 }
 
 template <int M, bool XM>
-static void adj_zl(int ZL, const AdjArgs& a, cudaStream_t st) {
+static void adj_zl(int ZL, const AdjArgs& a, int nzt, cudaStream_t st) {
   switch (ZL) {
-    case 8: adj_go<M, 8, XM>(a, st); break;
-    case 4: adj_go<M, 4, XM>(a, st); break;
-    case 2: adj_go<M, 2, XM>(a, st); break;
-    default: adj_go<M, 1, XM>(a, st); break;
+    case 8: adj_go<M, 8, XM>(a, nzt, st); break;
+    case 4: adj_go<M, 4, XM>(a, nzt, st); break;
+    case 2: adj_go<M, 2, XM>(a, nzt, st); break;
+    default: adj_go<M, 1, XM>(a, nzt, st); break;
   }
 }
 
@@ -442,17 +466,21 @@ static void adj_zl(int ZL, const AdjArgs& a, cudaStream_t st) {
 // others) through p.d_tmp.  order/counts come from launch_view_order.
 int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2* fc,
                 const int* order, const int* counts, int PN, const BackEpi& epi, cudaStream_t st) {
+  int zt0 = 0, nzt = 0;
+  ztile_range(p, epi.zlo, epi.zhi, &zt0, &nzt);
+  if (nzt == 0) return DDFAN_OK;
   if (back_mode == DDFAN_BACK_REF) {
     RefArgs a;
     a.satq = p.d_satq; a.vg = vg; a.PN = PN; a.U = p.U; a.Z = p.Z; a.ZB = p.ZB;
     a.XN = p.XN; a.YN = p.YN; a.ocx = p.ocx; a.ocy = p.ocy; a.dx = p.dx;
     a.inv_sid = p.inv_sid; a.inv_dbeta = p.inv_dbeta; a.cnt = (double)p.detCntIdx + 0.5;
     a.epi = epi;
+    a.zt0 = zt0;
     ProfScope ps(KIND_BACK_A, st);
     switch (p.mode) {
-      case SAT_FP32: ref_zl<SAT_FP32>(p.ZL, a, st); break;
-      case SAT_HILO: ref_zl<SAT_HILO>(p.ZL, a, st); break;
-      default: ref_zl<SAT_FP64>(p.ZL, a, st); break;
+      case SAT_FP32: ref_zl<SAT_FP32>(p.ZL, a, nzt, st); break;
+      case SAT_HILO: ref_zl<SAT_HILO>(p.ZL, a, nzt, st); break;
+      default: ref_zl<SAT_FP64>(p.ZL, a, nzt, st); break;
     }
     return check_launch("k_back_ref");
   }
@@ -465,6 +493,7 @@ int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2*
   a.t0 = p.t0; a.invdt = p.invdt; a.dirt = p.dirt; a.M = p.M;
   a.PN = PN; a.U = p.U; a.Z = p.Z; a.ZB = p.ZB; a.XN = p.XN; a.YN = p.YN;
   a.ocx = p.ocx; a.ocy = p.ocy; a.dx = p.dx;
+  a.zt0 = zt0;
   // pass 1: x-major views, lines = x columns -> tmp (mask applied)
   a.epi = epi;
   a.epi.out = p.d_tmp; a.epi.addend = nullptr; a.epi.xin = nullptr; a.epi.colsum = nullptr;
@@ -472,9 +501,9 @@ int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2*
   {
     ProfScope ps(KIND_BACK_A, st);
     switch (p.mode) {
-      case SAT_FP32: adj_zl<SAT_FP32, true>(p.ZL, a, st); break;
-      case SAT_HILO: adj_zl<SAT_HILO, true>(p.ZL, a, st); break;
-      default: adj_zl<SAT_FP64, true>(p.ZL, a, st); break;
+      case SAT_FP32: adj_zl<SAT_FP32, true>(p.ZL, a, nzt, st); break;
+      case SAT_HILO: adj_zl<SAT_HILO, true>(p.ZL, a, nzt, st); break;
+      default: adj_zl<SAT_FP64, true>(p.ZL, a, nzt, st); break;
     }
   }
   int rc = check_launch("k_back_adj<x>");
@@ -485,9 +514,9 @@ int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2*
   {
     ProfScope ps(KIND_BACK_B, st);
     switch (p.mode) {
-      case SAT_FP32: adj_zl<SAT_FP32, false>(p.ZL, a, st); break;
-      case SAT_HILO: adj_zl<SAT_HILO, false>(p.ZL, a, st); break;
-      default: adj_zl<SAT_FP64, false>(p.ZL, a, st); break;
+      case SAT_FP32: adj_zl<SAT_FP32, false>(p.ZL, a, nzt, st); break;
+      case SAT_HILO: adj_zl<SAT_HILO, false>(p.ZL, a, nzt, st); break;
+      default: adj_zl<SAT_FP64, false>(p.ZL, a, nzt, st); break;
     }
   }
   return check_launch("k_back_adj<y>");
@@ -500,7 +529,7 @@ int proj_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const floa
   int rc;
   if ((rc = launch_view_geom(p, d_angs, stride, PN, p.d_vg, p.d_fc, p.d_cvd, st))) return rc;
   if ((rc = launch_view_order(p.d_vg, PN, p.d_order, p.d_counts, st))) return rc;
-  if ((rc = launch_sat_image(p, d_vol, st))) return rc;
+  if ((rc = launch_sat_image(p, d_vol, st, zlo, zhi))) return rc;
   rc = launch_fwd(p, p.d_vg, p.d_fc, p.d_cvd, p.d_order, PN, d_prj, zlo, zhi, st);
   mark_use(p, st);
   return rc;
@@ -512,7 +541,8 @@ int back_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const floa
   if ((rc = launch_view_geom(p, d_angs, stride, PN, p.d_vg, p.d_fc, p.d_cvd, st))) return rc;
   if ((rc = launch_view_order(p.d_vg, PN, p.d_order, p.d_counts, st))) return rc;
   const bool adj = back_mode == DDFAN_BACK_ADJ;
-  if ((rc = launch_sat_sino(p, d_prj, PN, adj ? p.d_cvd : nullptr, 1.f, nullptr, nullptr, nullptr, st)))
+  if ((rc = launch_sat_sino(p, d_prj, PN, adj ? p.d_cvd : nullptr, 1.f, nullptr, nullptr, nullptr, st, zlo,
+                            zhi)))
     return rc;
   BackEpi e{};
   e.out = d_vol; e.mask = p.has_mask ? p.d_mask : nullptr; e.zlo = zlo; e.zhi = zhi;

@@ -101,6 +101,7 @@ struct SatSrc {
   const float* rowsum;  // [lines][U] row sums (slice 0) of the subset
   int XN, YN, U, Z;
   int ZLt;              // z-blocks per z-tile of the output layout
+  int zb0, zb1;         // z-blocks built: [zb0, zb1); grid y covers them 8 at a time
 };
 
 __device__ __forceinline__ void sat_load(const SatSrc& s, int line, int k, int zb,
@@ -166,8 +167,8 @@ __global__ void __launch_bounds__(512) k_sat(SatSrc s, float4* __restrict__ out,
   const int N = which ? N1 : N0, Nw = which ? Nw1 : Nw0;
   const int zl = threadIdx.x & 7, kc = threadIdx.x >> 3;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int zb = blockIdx.y * 8 + zl;
-  const bool zok = zb < ZB;
+  const int zb = s.zb0 + blockIdx.y * 8 + zl;
+  const bool zok = zb < s.zb1 && zb < ZB;
   const int k0 = kc * C;
   float v[C][4];
   Acc4<M> acc;

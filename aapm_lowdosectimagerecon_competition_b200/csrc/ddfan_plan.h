@@ -72,9 +72,14 @@ void plan_free(Plan* p);
 
 int launch_view_geom(const Plan& p, const float* d_angs, int stride, int PN, ViewGeom* vg,
                      double2* fc, float* cvd, cudaStream_t st);
-int launch_sat_image(const Plan& p, const float* d_vol, cudaStream_t st);
+// The prefix-sum builders, the forward projector and the backprojector run
+// only the z-blocks / z-tiles that hold slices [zlo, zhi) (zhi < 0: all);
+// slices outside the range that share a block are computed but not written
+// by the projectors.
+int launch_sat_image(const Plan& p, const float* d_vol, cudaStream_t st, int zlo = 0, int zhi = -1);
 int launch_sat_sino(const Plan& p, const float* d_prj, int PN, const float* wgt, float wscale,
-                    const float* y, const int* yview, const float* rowsum, cudaStream_t st);
+                    const float* y, const int* yview, const float* rowsum, cudaStream_t st, int zlo = 0,
+                    int zhi = -1);
 int launch_fwd(const Plan& p, const ViewGeom* vg, const double2* fc, const float* cvd,
                const int* order, int PN, float* d_prj, int zlo, int zhi, cudaStream_t st);
 int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2* fc,

@@ -61,7 +61,8 @@ struct FwdArgs {
   float* out;          // [PN][U][Z]
   int PN, U, Z, ZB, XN, YN;
   float dx;
-  int zlo, zhi;
+  int zlo, zhi;        // slices written
+  int zt0;             // z-tile of grid z-index 0 (the grid covers the tiles of [zlo, zhi))
 };
 
 template <int ZL, int CG>
@@ -90,7 +91,8 @@ __global__ void __launch_bounds__(256, 4) k_fwd(FwdArgs a) {
   const int tid = threadIdx.x;
   const int zl = tid % ZL, g = tid / ZL;
   const int p = a.order ? a.order[blockIdx.y] : blockIdx.y;
-  const int zb = blockIdx.z * ZL + zl;
+  const int zt = blockIdx.z + a.zt0;
+  const int zb = zt * ZL + zl;
   const int ub0 = blockIdx.x * CW;
   const bool xm = a.vg[p].xmajor != 0;
   const int nl = xm ? a.XN : a.YN, N = xm ? a.YN : a.XN;
@@ -99,7 +101,7 @@ __global__ void __launch_bounds__(256, 4) k_fwd(FwdArgs a) {
   for (int b = tid; b < NB; b += NT) s_fc[b] = a.fc[(size_t)p * (a.U + 1) + min(ub0 + b, a.U)];
   const bool active = (ub0 + g * CG < a.U) && (zb < a.ZB);
   // plane 0 of this lane's block in row 0 (see the table layout in ddfan_device.cuh)
-  const float4* base = sat + (size_t)(active ? blockIdx.z * ZL : 0) * F4 + zl;
+  const float4* base = sat + (size_t)(active ? zt * ZL : 0) * F4 + zl;
   // ray sums: each chunk of CC lines is summed into a fresh FP32 partial that
   // is then added to the total, so a 512-line sum rounds like ~sqrt(512/CC)
   // terms instead of 512
@@ -231,6 +233,7 @@ struct RefArgs {
   int PN, U, Z, ZB, XN, YN;
   double ocx, ocy, dx, inv_sid, inv_dbeta, cnt;  // cnt = detCntIdx + 1 - 0.5
   BackEpi epi;
+  int zt0;  // z-tile of grid z-index 0
 };
 
 // Reference backprojector formula (AAPM_script/MultiSlicesBackGPU.cu:115-184):
@@ -251,7 +254,8 @@ __global__ void __launch_bounds__(256, 3) k_back_ref(RefArgs a) {
   __shared__ int s_p[VC];
   const int tid = threadIdx.x;
   const int zl = tid % ZL, g = tid / ZL;
-  const int zb = blockIdx.z * ZL + zl;
+  const int zt = blockIdx.z + a.zt0;
+  const int zb = zt * ZL + zl;
   const int ntx = (a.XN + KT - 1) / KT;
   const int ty = blockIdx.x / ntx, tx = blockIdx.x - ty * ntx;
   const int y0 = ty * LT, x0 = tx * KT;
@@ -296,7 +300,7 @@ __global__ void __launch_bounds__(256, 3) k_back_ref(RefArgs a) {
     __syncthreads();
     if (active) {
       for (int vv = 0; vv < nvc; ++vv) {
-        const float4* base = a.satq + ((size_t)s_p[vv] * (a.U + 1) * a.ZB + blockIdx.z * ZL) * F4 + zl;
+        const float4* base = a.satq + ((size_t)s_p[vv] * (a.U + 1) * a.ZB + (size_t)zt * ZL) * F4 + zl;
 #pragma unroll
         for (int v = 0; v < VG; ++v) {
           const int r = l * KT + sg * VG + v;
@@ -334,6 +338,7 @@ struct AdjArgs {
   int PN, U, Z, ZB, XN, YN;
   double ocx, ocy, dx;
   BackEpi epi;
+  int zt0;  // z-tile of grid z-index 0
 };
 
 // Exact transpose of k_fwd.  For a view integrated along lines ii, pixel k of
@@ -361,7 +366,8 @@ __global__ void __launch_bounds__(256, 4) k_back_adj(AdjArgs a) {
   __shared__ uint16_t s_lut[LUTMAX];
   const int tid = threadIdx.x;
   const int zl = tid % ZL, g = tid / ZL;
-  const int zb = blockIdx.z * ZL + zl;
+  const int zt = blockIdx.z + a.zt0;
+  const int zb = zt * ZL + zl;
   const int nl = XM ? a.XN : a.YN, N = XM ? a.YN : a.XN;
   const int ntk = (N + KT - 1) / KT;
   const int tl = blockIdx.x / ntk, tk = blockIdx.x - tl * ntk;
@@ -424,7 +430,7 @@ __global__ void __launch_bounds__(256, 4) k_back_adj(AdjArgs a) {
     __syncthreads();
     if (active) {
       for (int vv = 0; vv < nvc; ++vv) {
-        const float4* base = a.satq + ((size_t)s_p[vv] * (a.U + 1) * a.ZB + blockIdx.z * ZL) * F4 + zl;
+        const float4* base = a.satq + ((size_t)s_p[vv] * (a.U + 1) * a.ZB + (size_t)zt * ZL) * F4 + zl;
         const float sgn = s_sgn[vv];
         // edges sg*VG .. sg*VG + VG of line l (the last one sits after a pad slot)
         const int2* geo = &s_geo[vv][l * LS + sg * (VG + 1)];

@@ -19,6 +19,7 @@
 // kernels evaluate those two once per row.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <vector>
 
@@ -84,15 +85,29 @@ __device__ __forceinline__ float rebin_view_angle(const RebinParams& p, int s, i
   return lam;
 }
 
-// one output sample of a valid row
+// one output sample of a valid row.  VEC: detector columns start 16-byte
+// aligned (DetHeight % 4 == 0); the two rows then come from one 16-byte load
+// (one L1 request per sample instead of two), plus a 4-byte load when they
+// straddle two 16-byte words.
+template <bool VEC>
 __device__ __forceinline__ float rebin_sample(const RebinParams& p, const RebinRow& r, int j) {
   float v;
   const float dv = rebin_dv(p, r.n, __ldg(p.sm + j), &v);
   int idv = (int)floorf(dv);
   idv = min(max(idv, 1), p.H - 1);  // already so for a valid row; keeps the loads in bounds regardless
   const float t = __fsub_rn(dv, (float)idv);
-  const float* c = r.col + (size_t)j * p.H + (idv - 1);
-  const float d0 = __ldg(c), d1 = __ldg(c + 1);
+  const float* colj = r.col + (size_t)j * p.H;
+  float d0, d1;
+  if (VEC) {
+    // e + 3 <= H - 1 because idv - 1 <= H - 2 and H % 4 == 0
+    const int e = (idv - 1) & ~3, q = (idv - 1) - e;
+    const float4 w = __ldg(reinterpret_cast<const float4*>(colj + e));
+    d0 = q == 0 ? w.x : q == 1 ? w.y : q == 2 ? w.z : w.w;
+    d1 = q == 0 ? w.y : q == 1 ? w.z : q == 2 ? w.w : __ldg(colj + e + 4);
+  } else {
+    d0 = __ldg(colj + idv - 1);
+    d1 = __ldg(colj + idv);
+  }
   const float temp = __fadd_rn(__fmul_rn(d0, __fsub_rn(1.0f, t)), __fmul_rn(d1, t));
   const float cosv = __fdiv_rn(p.SD, __fsqrt_rn(__fadd_rn(p.SD2, __fmul_rn(v, v))));
   return __fmul_rn(cosv, temp);
@@ -103,6 +118,7 @@ constexpr int kRowsPerCta = 8;  // one warp per output row
 // Reference (mex) layout: out[s][ib][j], views[s][ib].  One warp per row,
 // lanes over channels: coalesced stores; each sample loads two adjacent rows
 // of one detector column.
+template <bool VEC>
 __global__ void __launch_bounds__(256) k_rebin_mex(RebinParams p) {
   const int lane = threadIdx.x & 31;
   const int ib = blockIdx.x * kRowsPerCta + (threadIdx.x >> 5);
@@ -111,7 +127,16 @@ __global__ void __launch_bounds__(256) k_rebin_mex(RebinParams p) {
   const RebinRow r = rebin_row(p, s, ib);
   float* o = p.out + ((size_t)s * p.T + ib) * p.W;
   if (r.ok) {
-    for (int j = lane; j < p.W; j += 32) o[j] = rebin_sample(p, r, j);
+    // four channels per lane in flight
+    int j = lane;
+    for (; j + 96 < p.W; j += 128) {
+      float x[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) x[q] = rebin_sample<VEC>(p, r, j + 32 * q);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) o[j + 32 * q] = x[q];
+    }
+    for (; j < p.W; j += 32) o[j] = rebin_sample<VEC>(p, r, j);
   } else {
     for (int j = lane; j < p.W; j += 32) o[j] = 0.f;
   }
@@ -122,6 +147,7 @@ __global__ void __launch_bounds__(256) k_rebin_mex(RebinParams p) {
 // sinogram layout): out[ib][j][s], views[ib][s].  A CTA owns 32 slices of one
 // view; warps compute rows (lanes over 32 channels) into a shared tile, then
 // store it transposed with lanes over slices (128-byte rows).
+template <bool VEC>
 __global__ void __launch_bounds__(256) k_rebin_routine(RebinParams p) {
   __shared__ float tile[32][33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -146,7 +172,7 @@ __global__ void __launch_bounds__(256) k_rebin_routine(RebinParams p) {
     const int j = j0 + lane;
 #pragma unroll
     for (int q = 0; q < 4; ++q)
-      tile[warp * 4 + q][lane] = (rows[q].ok && j < p.W) ? rebin_sample(p, rows[q], j) : 0.f;
+      tile[warp * 4 + q][lane] = (rows[q].ok && j < p.W) ? rebin_sample<VEC>(p, rows[q], j) : 0.f;
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -226,13 +252,16 @@ int rebin_prepare(RebinHost& h, long long nViews, const float* zPos, int SLN, fl
 }
 
 int rebin_launch(const RebinParams& p, int layout, cudaStream_t st) {
+  // 16-byte loads need 16-byte aligned columns: DetHeight % 4 == 0 and an aligned base
+  const bool vec = p.H % 4 == 0 && (reinterpret_cast<uintptr_t>(p.raw) & 15) == 0;
   if (layout == 0) {
     dim3 grid((p.T + kRowsPerCta - 1) / kRowsPerCta, p.SLN);
-    k_rebin_mex<<<grid, 256, 0, st>>>(p);
+    if (vec) k_rebin_mex<true><<<grid, 256, 0, st>>>(p);
+    else k_rebin_mex<false><<<grid, 256, 0, st>>>(p);
   } else {
-    if (p.T > 0x7fffffff) return set_err(DDFAN_ERR_ARG, "HelicalToFan: DefTimes too large");
     dim3 grid(p.T, (p.SLN + 31) / 32);
-    k_rebin_routine<<<grid, 256, 0, st>>>(p);
+    if (vec) k_rebin_routine<true><<<grid, 256, 0, st>>>(p);
+    else k_rebin_routine<false><<<grid, 256, 0, st>>>(p);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "HelicalToFan launch: %s", cudaGetErrorString(e));
