@@ -51,6 +51,24 @@ class Scan:
         a = self.angles(PN)
         return np.repeat(a[:, None], self.SLN, axis=1)
 
+    def rebinned_hangs(self, spacing=36, BV=0.0):
+        """Per-slice view angles (PN, SLN) as helical rebinning leaves them:
+        slice z starts at raw view 1 + spacing * z and its view ib has angle
+        mod((start + ib - 1) * delta + BV, 2 pi) in float32
+        (AAPM_script/HelicalToFanFunc_mex.cpp:77-81) -- one grid, circularly
+        shifted per slice, different in the last bits from slice to slice."""
+        f = np.float32
+        delta, twopi = f(2.0 * math.pi / self.PN), f(2.0 * math.pi)
+        i = (np.arange(self.PN)[:, None] + spacing * np.arange(self.SLN)[None, :]).astype(np.float32)
+        lam = (i * delta).astype(np.float32) + f(BV)
+        # the reference's repeated float subtraction of 2 pi
+        while True:
+            over = lam > twopi
+            if not over.any():
+                break
+            lam = np.where(over, (lam - twopi).astype(np.float32), lam)
+        return lam.astype(np.float32)
+
     def circular_mask(self):
         """Disk mask of AAPM_script/reconscript.m:28-38 (radius 1.3 of the half
         width, i.e. nearly everything), as (YN, XN) bytes."""

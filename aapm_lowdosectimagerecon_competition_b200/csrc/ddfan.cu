@@ -195,6 +195,8 @@ int plan_create(Plan** out, const PlanDesc& d) {
     const int v = atoi(zl);
     if ((v == 1 || v == 2 || v == 4 || v == 8) && v <= p.ZL) p.ZL = v;
   }
+  if (d.zl_cap > 0)
+    while (p.ZL > 1 && p.ZL > d.zl_cap) p.ZL >>= 1;
   p.ZB = (p.ZB + p.ZL - 1) / p.ZL * p.ZL;  // whole z-tiles (padding blocks hold zeros)
   p.x0 = d.x0; p.y0 = d.y0; p.dx = d.dx; p.detCntIdx = d.detCntIdx;
   p.ocx = (d.XN - 1.0) * 0.5 - (double)d.imgXCenter / (double)d.dx;

@@ -25,6 +25,7 @@ struct PlanDesc {
   float dx;
   const uint8_t* mask;
   int SLN, PNmax, sat_mode, device;
+  int zl_cap = 0;  // > 0: at most this many z-blocks per z-tile (short slice ranges per launch)
 };
 
 // Geometry and device scratch for one (image, detector, slice count) shape.

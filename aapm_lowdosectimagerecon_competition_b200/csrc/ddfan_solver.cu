@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <unordered_map>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -65,6 +66,36 @@ void gather_slab(const float* src, size_t rows, int SLN, int a, int b, std::vect
 void scatter_slab(const std::vector<float>& src, size_t rows, int SLN, int a, int b, float* dst) {
   const int n = b - a;
   for (size_t r = 0; r < rows; ++r) std::memcpy(dst + r * SLN + a, &src[r * n], sizeof(float) * n);
+}
+
+// Distinct angle lists among the slices of hangs[PN][SLN] (bitwise equal
+// columns): slice_list[z] = list of slice z, rep[l] = first slice of list l.
+void angle_lists(const float* hangs, int PN, int SLN, std::vector<int>& slice_list, std::vector<int>& rep) {
+  std::vector<uint64_t> h(SLN, 1469598103934665603ull);
+  for (int q = 0; q < PN; ++q) {
+    const uint32_t* row = reinterpret_cast<const uint32_t*>(hangs + (size_t)q * SLN);
+    for (int z = 0; z < SLN; ++z) h[z] = (h[z] ^ row[z]) * 1099511628211ull;
+  }
+  std::unordered_map<uint64_t, std::vector<int>> by_hash;
+  slice_list.assign(SLN, -1);
+  rep.clear();
+  for (int z = 0; z < SLN; ++z) {
+    std::vector<int>& cand = by_hash[h[z]];
+    for (int l : cand) {
+      bool same = true;
+      for (int q = 0; q < PN && same; ++q)
+        same = std::memcmp(&hangs[(size_t)q * SLN + z], &hangs[(size_t)q * SLN + rep[l]], sizeof(float)) == 0;
+      if (same) {
+        slice_list[z] = l;
+        break;
+      }
+    }
+    if (slice_list[z] < 0) {
+      slice_list[z] = (int)rep.size();
+      cand.push_back((int)rep.size());
+      rep.push_back(z);
+    }
+  }
 }
 
 int device_count() {
@@ -156,18 +187,28 @@ static int mex_call(bool forward, float x0, float y0, int DNU, const float* xds,
 
 // ====================================================================== solver
 
+// Slices [z0, z1) whose angle lists are all list `list`.
+struct Segment {
+  int z0, z1, list;
+};
+
 struct Solver {
   Plan* P = nullptr;  // SLN slices, PNmax = largest subset
   int device = 0;
   int PNall = 0, nsub = 1, useFISTA = 1, nonneg = 0, back_mode = DDFAN_BACK_REF;
   int XN = 0, YN = 0, U = 0, Z = 0;
   std::vector<int> off, cnt;  // subset k: rows [off[k], off[k] + cnt[k]) of the subset-ordered tables
-  ViewGeom* d_vg = nullptr;
-  double2* d_fc = nullptr;
-  float* d_cvd = nullptr;
+  // Distinct per-slice angle lists (hangs[PNall][SLN] columns): one set of
+  // view tables per list, PNall rows each; runs of consecutive slices with one
+  // list are segments, projected and backprojected by their own launches.
+  int nlists = 1;
+  std::vector<Segment> segs;
+  ViewGeom* d_vg = nullptr;  // [nlists][PNall], subset order
+  double2* d_fc = nullptr;   // [nlists][PNall][U+1]
+  float* d_cvd = nullptr;    // [nlists][PNall][U]
   int* d_yview = nullptr;  // subset-ordered row -> original view index
-  int* d_order = nullptr;  // per subset: views in dispatch order (x-major first)
-  int* d_counts = nullptr; // per subset: {x-major views, others}
+  int* d_order = nullptr;  // [nlists][PNall]: per subset, views in dispatch order (x-major first)
+  int* d_counts = nullptr; // [nlists][nsub][2]: per subset, {x-major views, others}
   float* d_rows = nullptr; // [PNall][U]   row sums, subset order
   float* d_cols = nullptr; // [nsub][YN][XN] column sums
   float* d_y = nullptr;    // [PNall][U][Z] measured sinogram, original order
@@ -215,28 +256,38 @@ static int salloc(Solver& s, T** p, size_t n) {
 }
 
 // One OS-SART iteration (AAPM_script/OSSART_AAPM.m:79-115) on stream st.
+// Segments run one after another: slices of a neighbouring segment that share
+// a z-block are computed by each segment's launches but written only by their
+// own, and each segment rebuilds the sinogram table it backprojects.
 static int solver_iteration(Solver& s, cudaStream_t st) {
   Plan& p = *s.P;
   int rc, n = 0;
   const bool adj = s.back_mode == DDFAN_BACK_ADJ;
+  const size_t P = (size_t)s.PNall;
   for (int k = 0; k < s.nsub; ++k) {
     const int o = s.off[k], c = s.cnt[k];
-    const ViewGeom* vg = s.d_vg + o;
-    const double2* fc = s.d_fc + (size_t)o * (s.U + 1);
-    const float* cvd = s.d_cvd + (size_t)o * s.U;
     // project the current image (:85)
     if ((rc = launch_sat_image(p, s.d_x, st))) return rc;
-    if ((rc = launch_fwd(p, vg, fc, cvd, s.d_order + o, c, s.d_ax, 0, s.Z, st))) return rc;
-    // residual (y - A x) / rowSum folded into the sinogram prefix sums (:86-88)
-    if ((rc = launch_sat_sino(p, s.d_ax, c, adj ? cvd : nullptr, 1.f, s.d_y, s.d_yview + o,
-                              s.d_rows + (size_t)o * s.U, st)))
-      return rc;
-    // backproject, divide by colSum, add, optional clamp (:91-97)
-    BackEpi e{};
-    e.out = s.d_x; e.xin = s.d_x; e.colsum = s.d_cols + (size_t)k * s.XN * s.YN;
-    e.nonneg = s.nonneg; e.mask = p.has_mask ? p.d_mask : nullptr; e.zlo = 0; e.zhi = s.Z;
-    if ((rc = launch_back(p, s.back_mode, vg, fc, s.d_order + o, s.d_counts + 2 * k, c, e, st))) return rc;
-    n += adj ? 5 : 4;
+    ++n;
+    for (const Segment& g : s.segs) {
+      const size_t r = (size_t)g.list * P + o;
+      const ViewGeom* vg = s.d_vg + r;
+      const double2* fc = s.d_fc + r * (s.U + 1);
+      const float* cvd = s.d_cvd + r * s.U;
+      const int* order = s.d_order + r;
+      if ((rc = launch_fwd(p, vg, fc, cvd, order, c, s.d_ax, g.z0, g.z1, st))) return rc;
+      // residual (y - A x) / rowSum folded into the sinogram prefix sums (:86-88)
+      if ((rc = launch_sat_sino(p, s.d_ax, c, adj ? cvd : nullptr, 1.f, s.d_y, s.d_yview + o,
+                                s.d_rows + (size_t)o * s.U, st, g.z0, g.z1)))
+        return rc;
+      // backproject, divide by colSum, add, optional clamp (:91-97)
+      BackEpi e{};
+      e.out = s.d_x; e.xin = s.d_x; e.colsum = s.d_cols + (size_t)k * s.XN * s.YN;
+      e.nonneg = s.nonneg; e.mask = p.has_mask ? p.d_mask : nullptr; e.zlo = g.z0; e.zhi = g.z1;
+      const int* counts = s.d_counts + ((size_t)g.list * s.nsub + k) * 2;
+      if ((rc = launch_back(p, s.back_mode, vg, fc, order, counts, c, e, st))) return rc;
+      n += adj ? 4 : 3;
+    }
   }
   if (s.useFISTA) {
     const size_t V = (size_t)s.XN * s.YN * s.Z;
@@ -262,30 +313,40 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
   if (numOfOS < 1 || numOfOS > PNall) return set_err(DDFAN_ERR_ARG, "numOfOS=%d outside [1, %d]", numOfOS, PNall);
   if (back_mode != DDFAN_BACK_REF && back_mode != DDFAN_BACK_ADJ)
     return set_err(DDFAN_ERR_ARG, "back_mode %d", back_mode);
-  // the device solver shares one angle list across slices
-  for (int q = 0; q < PNall; ++q)
-    for (int z = 1; z < SLN; ++z)
-      if (std::memcmp(&hangs[(size_t)q * SLN + z], &hangs[(size_t)q * SLN], sizeof(float)) != 0)
-        return set_err(DDFAN_ERR_UNSUPPORTED, "solver: view %d has per-slice angles", q);
+  if (SLN < 1 || PNall < 1) return set_err(DDFAN_ERR_ARG, "SLN=%d PNall=%d", SLN, PNall);
   std::unique_ptr<Solver, void (*)(Solver*)> S(new Solver(), solver_free);
   Solver& s = *S;
   s.device = device; s.PNall = PNall; s.nsub = numOfOS; s.useFISTA = useFISTA ? 1 : 0;
   s.nonneg = nonneg ? 1 : 0; s.back_mode = back_mode; s.XN = XN; s.YN = YN; s.U = DNU; s.Z = SLN;
+  // distinct angle lists (bitwise) and the slices' runs of them
+  std::vector<int> rep, slice_list(SLN);
+  angle_lists(hangs, PNall, SLN, slice_list, rep);
+  s.nlists = (int)rep.size();
+  int shortest = SLN;
+  for (int z = 0; z < SLN;) {
+    int e = z + 1;
+    while (e < SLN && slice_list[e] == slice_list[z]) ++e;
+    s.segs.push_back({z, e, slice_list[z]});
+    shortest = std::min(shortest, e - z);
+    z = e;
+  }
   // subsets k, k + numOfOS, ... (AAPM_script/OSSART_AAPM.m:60)
   std::vector<int> yview;
-  std::vector<float> angs;
   int PNmax = 0;
   for (int k = 0; k < numOfOS; ++k) {
     s.off.push_back((int)yview.size());
-    for (int v = k; v < PNall; v += numOfOS) {
-      yview.push_back(v);
-      angs.push_back(hangs[(size_t)v * SLN]);
-    }
+    for (int v = k; v < PNall; v += numOfOS) yview.push_back(v);
     s.cnt.push_back((int)yview.size() - s.off.back());
     PNmax = std::max(PNmax, s.cnt.back());
   }
+  const size_t P = (size_t)PNall, L = (size_t)s.nlists;
+  std::vector<float> angs(L * P);
+  for (size_t l = 0; l < L; ++l)
+    for (size_t r = 0; r < P; ++r) angs[l * P + r] = hangs[(size_t)yview[r] * SLN + rep[l]];
   PlanDesc d{x0, y0, DNU, xds, yds, detCntIdx, imgXCenter, imgYCenter, XN, YN, dx, mask, SLN, PNmax,
              sat_mode, device};
+  // z-tiles no wider than the shortest segment (a launch computes whole tiles)
+  if (s.segs.size() > 1) d.zl_cap = std::max(1, std::min(8, shortest / 4));
   int rc = plan_create(&s.P, d);
   if (rc) return rc;
   s.bytes = s.P->bytes;
@@ -293,26 +354,31 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
   const size_t V = (size_t)XN * YN * SLN;
   DDFAN_CK(cudaStreamCreateWithFlags(&s.own, cudaStreamNonBlocking));
   DDFAN_CK(cudaEventCreateWithFlags(&s.last_use, cudaEventDisableTiming));
-  if ((rc = salloc(s, &s.d_vg, PNall)) || (rc = salloc(s, &s.d_fc, (size_t)PNall * (DNU + 1))) ||
-      (rc = salloc(s, &s.d_cvd, (size_t)PNall * DNU)) || (rc = salloc(s, &s.d_yview, PNall)) ||
-      (rc = salloc(s, &s.d_order, PNall)) || (rc = salloc(s, &s.d_counts, 2 * (size_t)numOfOS)) || (rc = salloc(s, &s.d_rows, (size_t)PNall * DNU)) ||
+  if ((rc = salloc(s, &s.d_vg, L * P)) || (rc = salloc(s, &s.d_fc, L * P * (DNU + 1))) ||
+      (rc = salloc(s, &s.d_cvd, L * P * DNU)) || (rc = salloc(s, &s.d_yview, PNall)) ||
+      (rc = salloc(s, &s.d_order, L * P)) || (rc = salloc(s, &s.d_counts, L * 2 * (size_t)numOfOS)) ||
+      (rc = salloc(s, &s.d_rows, (size_t)PNall * DNU)) ||
       (rc = salloc(s, &s.d_cols, (size_t)numOfOS * XN * YN)) ||
       (rc = salloc(s, &s.d_y, (size_t)PNall * DNU * SLN)) || (rc = salloc(s, &s.d_x, V)) ||
       (rc = salloc(s, &s.d_xprev, V)) || (rc = salloc(s, &s.d_ax, (size_t)PNmax * DNU * SLN)) ||
       (rc = salloc(s, &s.d_t, 1)))
     return rc;
   cudaStream_t st = s.own;
-  // per-view tables for every view, in subset order
+  // per-view tables for every view of every list, in subset order
   DevBuf<float> dang(st);
-  if ((rc = dang.alloc(PNall))) return rc;
-  DDFAN_CK(cudaMemcpyAsync(dang.p, angs.data(), sizeof(float) * PNall, cudaMemcpyHostToDevice, st));
+  if ((rc = dang.alloc(L * P))) return rc;
+  DDFAN_CK(cudaMemcpyAsync(dang.p, angs.data(), sizeof(float) * L * P, cudaMemcpyHostToDevice, st));
   DDFAN_CK(cudaMemcpyAsync(s.d_yview, yview.data(), sizeof(int) * PNall, cudaMemcpyHostToDevice, st));
-  if ((rc = launch_view_geom(*s.P, dang.p, 1, PNall, s.d_vg, s.d_fc, s.d_cvd, st))) return rc;
-  // per subset: views of one orientation together (one image table at a
-  // time stays hot in L2; the exact adjoint visits each orientation in turn)
-  for (int k = 0; k < numOfOS; ++k)
-    if ((rc = launch_view_order(s.d_vg + s.off[k], s.cnt[k], s.d_order + s.off[k], s.d_counts + 2 * k, st)))
-      return rc;
+  if ((rc = launch_view_geom(*s.P, dang.p, 1, (int)(L * P), s.d_vg, s.d_fc, s.d_cvd, st))) return rc;
+  // per list and subset: views of one orientation together (one image table
+  // at a time stays hot in L2; the exact adjoint visits each orientation in turn)
+  for (size_t l = 0; l < L; ++l)
+    for (int k = 0; k < numOfOS; ++k)
+      if ((rc = launch_view_order(s.d_vg + l * P + s.off[k], s.cnt[k], s.d_order + l * P + s.off[k],
+                                  s.d_counts + (l * numOfOS + k) * 2, st)))
+        return rc;
+  // the weights use slice 0's angles (AAPM_script/OSSART_AAPM.m:61-64)
+  const size_t l0 = (size_t)slice_list[0] * P;
   // row / column sums from slice 0 on a one-slice plan (AAPM_script/OSSART_AAPM.m:59-66)
   {
     PlanDesc d1 = d;
@@ -326,23 +392,25 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
     DDFAN_CK(cudaMemcpyAsync(ones.p, h1.data(), sizeof(float) * n1, cudaMemcpyHostToDevice, st));
     if ((rc = launch_sat_image(*P1.p, ones.p, st))) return rc;
     for (int k = 0; k < numOfOS; ++k) {
-      const int o = s.off[k], c = s.cnt[k];
-      if ((rc = launch_fwd(*P1.p, s.d_vg + o, s.d_fc + (size_t)o * (DNU + 1), s.d_cvd + (size_t)o * DNU,
-                           s.d_order + o, c, s.d_rows + (size_t)o * DNU, 0, 1, st)))
+      const size_t o = l0 + s.off[k];
+      const int c = s.cnt[k];
+      if ((rc = launch_fwd(*P1.p, s.d_vg + o, s.d_fc + o * (DNU + 1), s.d_cvd + o * DNU, s.d_order + o, c,
+                           s.d_rows + (size_t)s.off[k] * DNU, 0, 1, st)))
         return rc;
     }
     for (int k = 0; k < numOfOS; ++k) {
-      const int o = s.off[k], c = s.cnt[k];
+      const size_t o = l0 + s.off[k];
+      const int c = s.cnt[k];
       const bool adj = back_mode == DDFAN_BACK_ADJ;
-      if ((rc = launch_sat_sino(*P1.p, ones.p, c, adj ? s.d_cvd + (size_t)o * DNU : nullptr, 1.f,
-                                nullptr, nullptr, nullptr, st)))
+      if ((rc = launch_sat_sino(*P1.p, ones.p, c, adj ? s.d_cvd + o * DNU : nullptr, 1.f, nullptr, nullptr,
+                                nullptr, st)))
         return rc;
       BackEpi e{};
       e.out = s.d_cols + (size_t)k * XN * YN;
       e.mask = P1.p->has_mask ? P1.p->d_mask : nullptr;
       e.zlo = 0; e.zhi = 1;
-      if ((rc = launch_back(*P1.p, back_mode, s.d_vg + o, s.d_fc + (size_t)o * (DNU + 1), s.d_order + o,
-                            s.d_counts + 2 * k, c, e, st)))
+      if ((rc = launch_back(*P1.p, back_mode, s.d_vg + o, s.d_fc + o * (DNU + 1), s.d_order + o,
+                            s.d_counts + ((size_t)slice_list[0] * numOfOS + k) * 2, c, e, st)))
         return rc;
     }
     DDFAN_CK(cudaStreamSynchronize(st));
@@ -525,7 +593,8 @@ DDFAN_API float* ddfan_ossart_image_ptr(ddfan_ossart* h) {
 DDFAN_API int ddfan_ossart_launches_per_iter(const ddfan_ossart* h) {
   const Solver* s = reinterpret_cast<const Solver*>(h);
   if (!s) return 0;
-  return s->nsub * (s->back_mode == DDFAN_BACK_ADJ ? 5 : 4) + (s->useFISTA ? 2 : 0);
+  const int per_seg = s->back_mode == DDFAN_BACK_ADJ ? 4 : 3;
+  return s->nsub * (1 + (int)s->segs.size() * per_seg) + (s->useFISTA ? 2 : 0);
 }
 
 DDFAN_API int ddfan_OSSART_AAPM(float x0, float y0, int DNU, const float* xds, const float* yds,

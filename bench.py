@@ -50,6 +50,10 @@ def parse():
     ap.add_argument("--config", default="c3", choices=["c3", "c4", "c5", "rebin"],
                     help="c3: the OS-SART contract line; c4: batched uneven reconstructions; "
                          "c5: Poisson-arrival serving")
+    ap.add_argument("--views", default="shared", choices=["shared", "rebinned"],
+                    help="c3: one angle list for all slices, or per-slice lists as rebinning makes them")
+    ap.add_argument("--rotations", type=int, default=10, help="rebin: rotations of raw views")
+    ap.add_argument("--rebin-slices", type=int, default=512, help="rebin: target slices")
     ap.add_argument("--instances", type=int, default=32)
     ap.add_argument("--window", type=float, default=20.0)
     ap.add_argument("--rate", type=float, default=20.0)
@@ -192,8 +196,8 @@ def run_rebin_reference(args):
     bounded sample of slices per step (rank 0 only)."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    p, TV, z = rebin_workload()
-    sample = 32
+    p, TV, z = rebin_workload(args.rotations, args.rebin_slices)
+    sample = min(32, z.size)
     # only the raw views the sampled slices read are generated
     proj = _rebin_host_raw(p, min(TV, rebin_last_view(p, z[:sample])))
     rebin_cpu_timing(proj, z, p, 2)
@@ -235,7 +239,7 @@ def run_rebin(args):
                                 device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    p, TV, z = rebin_workload()
+    p, TV, z = rebin_workload(args.rotations, args.rebin_slices)
     SLN, T, W, H = z.size, p["DefTimes"], p["DetWidth"], p["DetHeight"]
     g = torch.Generator(device=dev)
     g.manual_seed(11 + rank)
@@ -342,7 +346,7 @@ def run_rebin(args):
                        "seconds_per_call": te}
         del P, Vw
     if rank == 0 and world == 1 and not args.no_cpu:
-        sample = 32
+        sample = min(32, SLN)
         sec, kind, cores = rebin_cpu_timing(proj_h, z, p, sample)
         line["cpu_baseline"] = {"value": 1.0 / sec, "unit": REBIN_UNIT, "cores": cores, "kind": kind,
                                 "sample": "first %d of %d slices; the reference's thread split gives every "
@@ -402,6 +406,8 @@ def config_dict(s, args, n):
                         (s.XN, s.YN, s.SLN, s.PN, s.DNU, s.numOfOS),
             "image": [s.XN, s.YN, s.SLN], "views": s.PN, "channels": s.DNU, "subsets": s.numOfOS,
             "sat": args.sat, "back": args.back, "instances": n,
+            "view_angles": "per-slice lists as helical rebinning makes them" if getattr(args, "views", "shared")
+                           == "rebinned" else "one list shared by all slices",
             "l2": "inputs larger than L2 (sinogram 868 MB, image 134 MB, prefix-sum tables 0.8 GB)",
             "parallelism": "one independent reconstruction per GPU (slices/requests shard with no exchange)"}
 
@@ -571,7 +577,8 @@ def run_ours(args):
     s = workload(args.slices)
     (x0, y0, xds, yds), xt, y = make_problem(s, dev, seed=7 + rank)
     mask = s.circular_mask()
-    solver = device.OSSART(x0, y0, s.DNU, xds, yds, s.detCntIdx, s.hangs(), s.XN, s.YN, s.SLN, s.dx,
+    hangs = s.rebinned_hangs() if args.views == "rebinned" else s.hangs()
+    solver = device.OSSART(x0, y0, s.DNU, xds, yds, s.detCntIdx, hangs, s.XN, s.YN, s.SLN, s.dx,
                            mask=mask, numOfOS=s.numOfOS, useFISTA=s.useFISTA, nonneg=s.nonneg,
                            sat=args.sat, back=args.back, device=local)
     solver.set_sinogram(y)
@@ -684,7 +691,7 @@ def _ossart_host(s, geom, y_h, x_h, out_h, mask, iters, args):
     import ctypes
     from aapm_lowdosectimagerecon_competition_b200._lib import BACK_MODES, SAT_MODES, call
     x0, y0, xds, yds = geom
-    hangs = np.ascontiguousarray(s.hangs())
+    hangs = np.ascontiguousarray(s.rebinned_hangs() if args.views == "rebinned" else s.hangs())
     m = np.ascontiguousarray(mask, np.uint8)
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
     T = lambda t: ctypes.c_void_p(t.data_ptr())

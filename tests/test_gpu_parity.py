@@ -199,6 +199,56 @@ def test_ossart_matches_oracle(mods, back, nonneg):
         assert x1.min() >= 0
 
 
+def rebinned_angles(PN, SLN, starts, BV=0.3):
+    """Per-slice view angles the way the helical rebinning makes them:
+    mod((start_s + ib - 1) * delta + BV, 2 pi) in float32 for slice s, view ib
+    (HelicalToFanFunc_mex.cpp:77-81) -- circular shifts of one grid that
+    differ from slice to slice in their last bits."""
+    f = np.float32
+    delta, twopi = f(2 * math.pi / PN), f(2 * math.pi)
+    h = np.zeros((PN, SLN), np.float32)
+    for z in range(SLN):
+        for ib in range(PN):
+            lam = f(f(starts[z] + ib) * delta) + f(BV)
+            while lam > twopi:
+                lam = f(lam - twopi)
+            h[ib, z] = lam
+    return h
+
+
+@pytest.mark.parametrize("back", ["ref", "adj"])
+@pytest.mark.parametrize("lists", ["rebinned", "repeating"])
+def test_ossart_per_slice_angles_matches_oracle(mods, back, lists):
+    """OSSART_AAPM with Views(SLN, PN) that differ per slice (the rebinned
+    real-data case): every slice is projected with its own angles and the
+    subset weights come from slice 0 (OSSART_AAPM.m:61-64)."""
+    dd2, configs, device, O = mods
+    SLN = 7
+    s = configs.scaled(configs.c3(SLN=SLN), XN=40, DNU=64, PN=96)
+    s.numOfOS = 6
+    x0, y0, xds, yds = dd2.fan_geometry(s.sid, s.sdd, s.DNU, s.detCellWidth, s.detCntIdx)
+    if lists == "rebinned":
+        h = rebinned_angles(s.PN, SLN, [37 * z + 5 for z in range(SLN)])
+    else:
+        # three lists over seven slices: segments A A | B | C | A | C C
+        base = rebinned_angles(s.PN, 3, [0, 11, 50])
+        h = base[:, [0, 0, 1, 2, 0, 2, 2]].copy()
+    xt = configs.phantom(s)
+    mask = s.circular_mask()
+    y = O.proj(x0, y0, s.DNU, xds, yds, 0, 0, h, s.PN, s.XN, s.YN, SLN, xt, s.dx, mask)
+    y = configs.poisson_log(y, 1.5e5, seed=5)
+    init = np.zeros_like(xt)
+    xg = dd2.OSSART_AAPM(y, h, init, s.conf(), 4, s.numOfOS, mask, 1, 0, sat="hilo", back=back)
+    xo = O.ossart(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0, 0, h, s.PN, s.XN, s.YN, SLN, y, init, s.dx, mask, 4,
+                  s.numOfOS, 1, 0, O.REF if back == "ref" else O.ADJ)
+    assert rel(xg, xo) < 1e-5
+    # a slice on its own is the same problem (weights from its own angles
+    # only matter for slice 0, which is kept first)
+    x_first = dd2.OSSART_AAPM(y[:, :, :1], h[:, :1], init[:, :, :1], dict(s.conf(), SLN=1), 4, s.numOfOS,
+                              mask, 1, 0, sat="hilo", back=back)
+    assert rel(xg[:, :, :1], x_first) < 1e-6
+
+
 def test_ossart_graph_equals_stream_launches(mods):
     import torch
     dd2, configs, device, O = mods
