@@ -195,8 +195,7 @@ int plan_create(Plan** out, const PlanDesc& d) {
     const int v = atoi(zl);
     if ((v == 1 || v == 2 || v == 4 || v == 8) && v <= p.ZL) p.ZL = v;
   }
-  if (d.zl_cap > 0)
-    while (p.ZL > 1 && p.ZL > d.zl_cap) p.ZL >>= 1;
+  if (d.zl_force == 1 || d.zl_force == 2 || d.zl_force == 4 || d.zl_force == 8) p.ZL = d.zl_force;
   p.ZB = (p.ZB + p.ZL - 1) / p.ZL * p.ZL;  // whole z-tiles (padding blocks hold zeros)
   p.x0 = d.x0; p.y0 = d.y0; p.dx = d.dx; p.detCntIdx = d.detCntIdx;
   p.ocx = (d.XN - 1.0) * 0.5 - (double)d.imgXCenter / (double)d.dx;
@@ -368,10 +367,13 @@ int launch_sat_image(const Plan& p, const float* d_vol, cudaStream_t st, int zlo
 
 int launch_sat_sino(const Plan& p, const float* d_prj, int PN, const float* wgt, float wscale,
                     const float* y, const int* yview, const float* rowsum, cudaStream_t st, int zlo,
-                    int zhi) {
+                    int zhi, const ViewRanges* vr) {
   SatSrc s{};
   s.kind = 2; s.a = d_prj; s.wgt = wgt; s.wscale = wscale; s.y = y; s.yview = yview;
   s.rowsum = rowsum; s.XN = p.XN; s.YN = p.YN; s.U = p.U; s.Z = p.Z; s.ZLt = p.ZL;
+  if (vr) {
+    s.ztd = vr->ztd; s.soff = vr->soff; s.Mc = vr->Mc; s.nOS = vr->nOS; s.ksub = vr->ksub; s.T = vr->T;
+  }
   zblock_range(p, zlo, zhi, &s.zb0, &s.zb1);
   if (s.zb1 <= s.zb0) return DDFAN_OK;
   ProfScope ps(KIND_SAT_SINO, st);
@@ -383,6 +385,13 @@ int launch_view_order(const ViewGeom* vg, int PN, int* order, int* counts, cudaS
   ProfScope ps(KIND_VIEW_GEOM, st);
   k_view_order<<<1, 1024, 0, st>>>(vg, PN, order, counts);
   return check_launch("k_view_order");
+}
+
+int launch_view_order_ranges(const ViewGeom* vg, int4* desc, int nr, int* order, cudaStream_t st) {
+  if (nr < 1) return DDFAN_OK;
+  ProfScope ps(KIND_VIEW_GEOM, st);
+  k_view_order_ranges<<<nr, 1024, 0, st>>>(vg, desc, order);
+  return check_launch("k_view_order_ranges");
 }
 
 // channels per thread of the forward projector for a z-lane count
@@ -407,9 +416,11 @@ static void fwd_zl(int ZL, const FwdArgs& a, int nzt, cudaStream_t st) {
 }
 
 int launch_fwd(const Plan& p, const ViewGeom* vg, const double2* fc, const float* cvd,
-               const int* order, int PN, float* d_prj, int zlo, int zhi, cudaStream_t st) {
+               const int* order, int PN, float* d_prj, int zlo, int zhi, cudaStream_t st,
+               const int4* ztd) {
   if (PN > 65535) return set_err(DDFAN_ERR_UNSUPPORTED, "more than 65535 views in one call");
   FwdArgs a;
+  a.ztd = ztd;
   a.satx = p.d_satx; a.saty = p.d_saty; a.vg = vg; a.fc = fc; a.cvd = cvd; a.order = order;
   a.out = d_prj; a.PN = PN; a.U = p.U; a.Z = p.Z; a.ZB = p.ZB; a.XN = p.XN; a.YN = p.YN;
   a.dx = p.dx; a.zlo = zlo; a.zhi = zhi;
@@ -467,7 +478,8 @@ static void adj_zl(int ZL, const AdjArgs& a, int nzt, cudaStream_t st) {
 // passes (x-column lines over the x-major views, then y-row lines over the
 // others) through p.d_tmp.  order/counts come from launch_view_order.
 int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2* fc,
-                const int* order, const int* counts, int PN, const BackEpi& epi, cudaStream_t st) {
+                const int* order, const int* counts, int PN, const BackEpi& epi, cudaStream_t st,
+                const int4* ztd) {
   int zt0 = 0, nzt = 0;
   ztile_range(p, epi.zlo, epi.zhi, &zt0, &nzt);
   if (nzt == 0) return DDFAN_OK;
@@ -478,6 +490,7 @@ int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2*
     a.inv_sid = p.inv_sid; a.inv_dbeta = p.inv_dbeta; a.cnt = (double)p.detCntIdx + 0.5;
     a.epi = epi;
     a.zt0 = zt0;
+    a.ztd = ztd;
     ProfScope ps(KIND_BACK_A, st);
     switch (p.mode) {
       case SAT_FP32: ref_zl<SAT_FP32>(p.ZL, a, nzt, st); break;
@@ -488,8 +501,9 @@ int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2*
   }
   if (back_mode != DDFAN_BACK_ADJ) return set_err(DDFAN_ERR_ARG, "back_mode %d", back_mode);
   if (!p.adj_ok) return set_err(DDFAN_ERR_UNSUPPORTED, "detector boundaries are not monotone as seen from the source");
-  if (!order || !counts) return set_err(DDFAN_ERR_ARG, "exact adjoint needs the view order");
+  if (!order || (!counts && !ztd)) return set_err(DDFAN_ERR_ARG, "exact adjoint needs the view order");
   AdjArgs a;
+  a.ztd = ztd;
   a.satq = p.d_satq; a.vg = vg; a.fc = fc; a.tb = p.d_tb; a.lut = p.d_lut;
   a.order = order; a.counts = counts;
   a.t0 = p.t0; a.invdt = p.invdt; a.dirt = p.dirt; a.M = p.M;

@@ -102,6 +102,14 @@ struct SatSrc {
   int XN, YN, U, Z;
   int ZLt;              // z-blocks per z-tile of the output layout
   int zb0, zb1;         // z-blocks built: [zb0, zb1); grid y covers them 8 at a time
+  // Per-slice view angles (solver): line = slot of the z-tile's view range
+  // ztd[zt] = {first geometry row, count, -, -}; geometry row r is raw view
+  // g = r / Mc + (r % Mc) * nOS; slice z reads its view g - soff[z] of y when
+  // that lies in [0, T) (else the residual is 0), with row sum row
+  // (view - ksub) / nOS.  Null ztd: lines are views (yview, rowsum by line).
+  const int4* ztd;
+  const int* soff;
+  int Mc, nOS, ksub, T;
 };
 
 __device__ __forceinline__ void sat_load(const SatSrc& s, int line, int k, int zb,
@@ -124,6 +132,33 @@ __device__ __forceinline__ void sat_load(const SatSrc& s, int line, int k, int z
   const int z0 = zb * 4;
   if (z0 >= s.Z) {  // padding block of the last z-tile
     v[0] = v[1] = v[2] = v[3] = 0.f;
+    return;
+  }
+  if (s.kind == 2 && s.ztd) {
+    const int4 d = s.ztd[zb / s.ZLt];
+    if (line >= d.y) {
+      v[0] = v[1] = v[2] = v[3] = 0.f;
+      return;
+    }
+    const int r = d.x + line;
+    const long long g = (long long)(r / s.Mc) + (long long)(r % s.Mc) * s.nOS;
+    const float mw = s.wgt ? __ldg(s.wgt + (size_t)r * s.U + k) * s.wscale : s.wscale;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int z = z0 + i;
+      float val = 0.f;
+      if (z < s.Z) {
+        const long long ib = g - (long long)__ldg(s.soff + z);
+        if (ib >= 0 && ib < s.T) {
+          const float ax = __ldg(s.a + base + z);
+          const float rs = __ldg(s.rowsum + (size_t)((ib - s.ksub) / s.nOS) * s.U + k);
+          const float yv = __ldg(s.y + ((size_t)ib * s.U + k) * s.Z + z);
+          // (y - A x) / rowSum where rowSum != 0, else A x (AAPM_script/OSSART_AAPM.m:88)
+          val = rs != 0.f ? __fdiv_rn(__fsub_rn(yv, ax), rs) : ax;
+        }
+      }
+      v[i] = val * mw;
+    }
     return;
   }
   if ((s.Z & 3) == 0) {

@@ -25,7 +25,7 @@ struct PlanDesc {
   float dx;
   const uint8_t* mask;
   int SLN, PNmax, sat_mode, device;
-  int zl_cap = 0;  // > 0: at most this many z-blocks per z-tile (short slice ranges per launch)
+  int zl_force = 0;  // 1, 2, 4 or 8: exactly this many z-blocks per z-tile (else chosen by pow2_zl)
 };
 
 // Geometry and device scratch for one (image, detector, slice count) shape.
@@ -78,14 +78,29 @@ int launch_view_geom(const Plan& p, const float* d_angs, int stride, int PN, Vie
 // slices outside the range that share a block are computed but not written
 // by the projectors.
 int launch_sat_image(const Plan& p, const float* d_vol, cudaStream_t st, int zlo = 0, int zhi = -1);
+// Per-slice view angles in the solver: each z-tile projects its own range of
+// geometry rows (ztd[zt] = {first row, count, slot-order offset, x-major
+// count}); row r is raw view r / Mc + (r % Mc) * nOS and slice z of the
+// sinogram y reads that raw view as its view (raw view - soff[z]) of T, in
+// subset ksub.  PN of the launches is then the largest count.
+struct ViewRanges {
+  const int4* ztd = nullptr;
+  const int* soff = nullptr;
+  int Mc = 1, nOS = 1, ksub = 0, T = 0;
+};
+
 int launch_sat_sino(const Plan& p, const float* d_prj, int PN, const float* wgt, float wscale,
                     const float* y, const int* yview, const float* rowsum, cudaStream_t st, int zlo = 0,
-                    int zhi = -1);
+                    int zhi = -1, const ViewRanges* vr = nullptr);
 int launch_fwd(const Plan& p, const ViewGeom* vg, const double2* fc, const float* cvd,
-               const int* order, int PN, float* d_prj, int zlo, int zhi, cudaStream_t st);
+               const int* order, int PN, float* d_prj, int zlo, int zhi, cudaStream_t st,
+               const int4* ztd = nullptr);
 int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2* fc,
-                const int* order, const int* counts, int PN, const BackEpi& epi, cudaStream_t st);
+                const int* order, const int* counts, int PN, const BackEpi& epi, cudaStream_t st,
+                const int4* ztd = nullptr);
 int launch_view_order(const ViewGeom* vg, int PN, int* order, int* counts, cudaStream_t st);
+// k_view_order over nr ranges (desc[r] = {first row, count, order offset, -> x-major count})
+int launch_view_order_ranges(const ViewGeom* vg, int4* desc, int nr, int* order, cudaStream_t st);
 int proj_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const float* d_vol,
                     float* d_prj, int zlo, int zhi, cudaStream_t st);
 int back_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const float* d_prj,

@@ -49,6 +49,64 @@ static __global__ void __launch_bounds__(1024) k_view_order(const ViewGeom* __re
   }
 }
 
+// The same partition for many view ranges at once (one CTA per range):
+// range r covers geometry rows [d.x, d.x + d.y); its slots 0..d.y-1 go to
+// order[d.z ...], x-major first, and d.w receives the x-major count.
+static __global__ void __launch_bounds__(1024) k_view_order_ranges(const ViewGeom* __restrict__ vg,
+                                                                   int4* __restrict__ desc,
+                                                                   int* __restrict__ order) {
+  __shared__ int sx[1024], sy[1024], tot;
+  const int4 d = desc[blockIdx.x];
+  const ViewGeom* v = vg + d.x;
+  int* o = order + d.z;
+  const int PN = d.y;
+  const int t = threadIdx.x, T = blockDim.x;
+  const int ch = (PN + T - 1) / T;
+  const int a = min(PN, t * ch), b = min(PN, a + ch);
+  int nx = 0;
+  for (int p = a; p < b; ++p) nx += v[p].xmajor != 0;
+  sx[t] = nx;
+  sy[t] = (b - a) - nx;
+  __syncthreads();
+  if (t == 0) {
+    int ax = 0, ay = 0;
+    for (int i = 0; i < T; ++i) {
+      const int u = sx[i], w = sy[i];
+      sx[i] = ax;
+      sy[i] = ay;
+      ax += u;
+      ay += w;
+    }
+    tot = ax;
+    desc[blockIdx.x].w = ax;
+  }
+  __syncthreads();
+  int ox = sx[t], oy = tot + sy[t];
+  for (int p = a; p < b; ++p) {
+    if (v[p].xmajor) o[ox++] = p;
+    else o[oy++] = p;
+  }
+}
+
+// Per z-tile view ranges (solver with per-slice view angles): tile zt
+// projects the views {x: first geometry row, y: count, z: offset of its slot
+// order, w: x-major count}; output rows and sinogram-table rows are the
+// tile's slots 0..count-1.  Null: every tile uses all PN views (rows = slots).
+struct ZtRange {
+  int gbase, count, ooff, nx;
+};
+
+__device__ __forceinline__ ZtRange zt_range(const int4* ztd, int zt, int PN, const int* counts) {
+  ZtRange r;
+  if (ztd) {
+    const int4 d = ztd[zt];
+    r.gbase = d.x; r.count = d.y; r.ooff = d.z; r.nx = d.w;
+  } else {
+    r.gbase = 0; r.count = PN; r.ooff = 0; r.nx = counts ? counts[0] : 0;
+  }
+  return r;
+}
+
 // ============================================================ forward projector
 
 struct FwdArgs {
@@ -63,6 +121,7 @@ struct FwdArgs {
   float dx;
   int zlo, zhi;        // slices written
   int zt0;             // z-tile of grid z-index 0 (the grid covers the tiles of [zlo, zhi))
+  const int4* ztd;     // per z-tile view ranges, or null
 };
 
 template <int ZL, int CG>
@@ -90,8 +149,11 @@ __global__ void __launch_bounds__(256, 4) k_fwd(FwdArgs a) {
   __shared__ float s_inv[CC][CW];  // 1 / (footprint length in mm)
   const int tid = threadIdx.x;
   const int zl = tid % ZL, g = tid / ZL;
-  const int p = a.order ? a.order[blockIdx.y] : blockIdx.y;
   const int zt = blockIdx.z + a.zt0;
+  const ZtRange rg = zt_range(a.ztd, zt, a.PN, nullptr);
+  if ((int)blockIdx.y >= rg.count) return;  // uniform per CTA
+  const int slot = a.order ? a.order[rg.ooff + blockIdx.y] : blockIdx.y;
+  const int p = rg.gbase + slot;  // geometry row
   const int zb = zt * ZL + zl;
   const int ub0 = blockIdx.x * CW;
   const bool xm = a.vg[p].xmajor != 0;
@@ -166,7 +228,7 @@ __global__ void __launch_bounds__(256, 4) k_fwd(FwdArgs a) {
     const int u = ub0 + g * CG + j;
     if (u >= a.U) break;
     const float cv = __ldg(a.cvd + (size_t)p * a.U + u) * dx;
-    float* o = a.out + ((size_t)p * a.U + u) * a.Z;
+    float* o = a.out + ((size_t)slot * a.U + u) * a.Z;
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
       const int z = zb * 4 + s;
@@ -234,6 +296,7 @@ struct RefArgs {
   double ocx, ocy, dx, inv_sid, inv_dbeta, cnt;  // cnt = detCntIdx + 1 - 0.5
   BackEpi epi;
   int zt0;  // z-tile of grid z-index 0
+  const int4* ztd;  // per z-tile view ranges, or null
 };
 
 // Reference backprojector formula (AAPM_script/MultiSlicesBackGPU.cu:115-184):
@@ -262,13 +325,14 @@ __global__ void __launch_bounds__(256, 3) k_back_ref(RefArgs a) {
   const int l = g / SPL, sg = g - l * SPL;
   const int iy = y0 + l, ixs = x0 + sg * VG;
   const bool active = zb < a.ZB && iy < a.YN && ixs < a.XN;
+  const ZtRange rg = zt_range(a.ztd, zt, a.PN, nullptr);
   float acc[VG][4];
 #pragma unroll
   for (int v = 0; v < VG; ++v) acc[v][0] = acc[v][1] = acc[v][2] = acc[v][3] = 0.f;
   const double Ud = (double)a.U;
   const size_t rowstride = (size_t)a.ZB * F4;
-  for (int v0 = 0; v0 < a.PN; v0 += VC) {
-    const int nvc = min(VC, a.PN - v0);
+  for (int v0 = 0; v0 < rg.count; v0 += VC) {
+    const int nvc = min(VC, rg.count - v0);
     if (tid < VC) s_p[tid] = v0 + tid;
     for (int e = tid; e < VC * NV; e += NT) {
       const int vv = e / NV, r = e - vv * NV;
@@ -279,7 +343,7 @@ __global__ void __launch_bounds__(256, 3) k_back_ref(RefArgs a) {
       float w = 0.f;
       if (vv < nvc && yy < a.YN && xx < a.XN &&
           (!a.epi.mask || a.epi.mask[(size_t)yy * a.XN + xx] != 0)) {
-        const ViewGeom& G = a.vg[v0 + vv];
+        const ViewGeom& G = a.vg[rg.gbase + v0 + vv];
         const double sx = G.sx, sy = G.sy;
         const double ddx = (xx - a.ocx) * a.dx - sx, ddy = (yy - a.ocy) * a.dx - sy;
         const double l2 = ddx * ddx + ddy * ddy;
@@ -339,6 +403,7 @@ struct AdjArgs {
   double ocx, ocy, dx;
   BackEpi epi;
   int zt0;  // z-tile of grid z-index 0
+  const int4* ztd;  // per z-tile view ranges (order, counts then unused), or null
 };
 
 // Exact transpose of k_fwd.  For a view integrated along lines ii, pixel k of
@@ -377,8 +442,10 @@ __global__ void __launch_bounds__(256, 4) k_back_adj(AdjArgs a) {
   const bool active = zb < a.ZB && ii < nl && ks < N;
   for (int i = tid; i <= a.U; i += NT) s_tb[i] = a.tb[i];
   for (int i = tid; i < a.M; i += NT) s_lut[i] = a.lut[i];
-  const int nx = a.counts[0];
-  const int vbeg = XM ? 0 : nx, vend = XM ? nx : a.PN;
+  const ZtRange rg = zt_range(a.ztd, zt, a.PN, a.counts);
+  const int* order = a.order + rg.ooff;
+  const int nx = rg.nx;
+  const int vbeg = XM ? 0 : nx, vend = XM ? nx : rg.count;
   float acc[VG][4];
 #pragma unroll
   for (int v = 0; v < VG; ++v) acc[v][0] = acc[v][1] = acc[v][2] = acc[v][3] = 0.f;
@@ -389,9 +456,9 @@ __global__ void __launch_bounds__(256, 4) k_back_adj(AdjArgs a) {
   for (int v0 = vbeg; v0 < vend; v0 += VC) {
     const int nvc = min(VC, vend - v0);
     if (tid < VC && tid < nvc) {
-      const int p = a.order[v0 + tid];
+      const int p = order[v0 + tid];
       s_p[tid] = p;
-      s_sgn[tid] = a.vg[p].sgn;
+      s_sgn[tid] = a.vg[rg.gbase + p].sgn;
     }
     for (int e = tid; e < VC * NE; e += NT) {
       const int vv = e / NE, r = e - vv * NE;
@@ -400,7 +467,7 @@ __global__ void __launch_bounds__(256, 4) k_back_adj(AdjArgs a) {
       int b = 0;
       float frac = 0.f;
       if (vv < nvc && li < nl && ck <= N) {
-        const int p = a.order[v0 + vv];
+        const int p = rg.gbase + order[v0 + vv];
         const ViewGeom& G = a.vg[p];
         const double lineX = (li - ocl) * a.dx, along = ((double)ck - 0.5 - ock) * a.dx;
         const float vx = (float)((XM ? lineX : along) - G.sx);

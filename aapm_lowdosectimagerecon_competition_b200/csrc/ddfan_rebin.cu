@@ -56,7 +56,7 @@ __device__ __forceinline__ bool rebin_in_rows(const RebinParams& p, float dv) {
 
 struct RebinRow {
   const float* col;  // raw view of this row, channel 0
-  float n;           // z - zz
+  float n;           // z - zz, zz = (i - 1) deltaZ the height of raw view i
   bool ok;           // computed and every channel inside the detector rows
 };
 
@@ -113,34 +113,72 @@ __device__ __forceinline__ float rebin_sample(const RebinParams& p, const RebinR
   return __fmul_rn(cosv, temp);
 }
 
-constexpr int kRowsPerCta = 8;  // one warp per output row
+constexpr int kDiagViews = 32;  // raw views per CTA of k_rebin_diag
 
-// Reference (mex) layout: out[s][ib][j], views[s][ib].  One warp per row,
-// lanes over channels: coalesced stores; each sample loads two adjacent rows
-// of one detector column.
+// Mex layout out[s][ib][j], views[s][ib], traversed along raw views: a CTA
+// owns 32 consecutive slices (one per lane) and 32 consecutive raw views
+// (4 per warp).  For raw view i, lane s produces row ib = i - start_s of its
+// slice, so the 32 lanes read one detector column at 32 neighbouring heights
+// (a few sectors per load instead of one sector per lane) and the slice
+// blocks that need view i run side by side and share it in L2.  Each warp
+// gathers a 32-slice x 32-channel tile in shared memory and stores it as
+// 128-byte row pieces.  Rows this traversal never visits (raw view < 1) are
+// written by k_rebin_unvisited.
 template <bool VEC>
-__global__ void __launch_bounds__(256) k_rebin_mex(RebinParams p) {
-  const int lane = threadIdx.x & 31;
-  const int ib = blockIdx.x * kRowsPerCta + (threadIdx.x >> 5);
-  const int s = blockIdx.y;
-  if (ib >= p.T) return;
-  const RebinRow r = rebin_row(p, s, ib);
-  float* o = p.out + ((size_t)s * p.T + ib) * p.W;
-  if (r.ok) {
-    // four channels per lane in flight
-    int j = lane;
-    for (; j + 96 < p.W; j += 128) {
-      float x[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) x[q] = rebin_sample<VEC>(p, r, j + 32 * q);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) o[j + 32 * q] = x[q];
+__global__ void __launch_bounds__(256) k_rebin_diag(RebinParams p, long long vlo, long long vhi) {
+  __shared__ float tile[8][32][33];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int s = blockIdx.x * 32 + lane;
+  const bool sok = s < p.SLN;
+  const int st = sok ? p.start[s] : -1;
+  const float z = sok ? p.zpos[s] : 0.f;
+  float(*t)[33] = tile[warp];
+  const long long i0 = vlo + (long long)blockIdx.y * kDiagViews;
+  for (int v = warp; v < kDiagViews; v += 8) {
+    const long long i = i0 + v;  // 1-based raw view, >= vlo >= 1
+    if (i > vhi) break;
+    const long long ibl = i - st;
+    const bool act = sok && st >= 0 && ibl >= 0 && ibl < p.T;
+    const unsigned amask = __ballot_sync(0xffffffffu, act);
+    if (!amask) continue;
+    const int ib = act ? (int)ibl : 0;
+    RebinRow r;
+    r.n = __fsub_rn(z, __fmul_rn((float)(i - 1), p.deltaZ));
+    float vtmp;
+    r.ok = act && rebin_in_rows(p, rebin_dv(p, r.n, p.sm_lo, &vtmp)) &&
+           rebin_in_rows(p, rebin_dv(p, r.n, p.sm_hi, &vtmp));
+    r.col = p.raw + (size_t)(i - p.view0) * p.W * p.H;
+    if (act) {
+      float lam = __fadd_rn(__fmul_rn((float)(i - 1), p.delta), p.BV);
+      while (lam > p.twopi) lam = __fsub_rn(lam, p.twopi);
+      p.views[(size_t)s * p.T + ib] = lam;
     }
-    for (; j < p.W; j += 32) o[j] = rebin_sample<VEC>(p, r, j);
-  } else {
-    for (int j = lane; j < p.W; j += 32) o[j] = 0.f;
+    for (int j0 = 0; j0 < p.W; j0 += 32) {
+      const int nc = min(32, p.W - j0);
+#pragma unroll 4
+      for (int c = 0; c < 32; ++c) t[lane][c] = (r.ok && c < nc) ? rebin_sample<VEC>(p, r, j0 + c) : 0.f;
+      __syncwarp();
+      for (unsigned m = amask; m; m &= m - 1) {
+        const int q = __ffs(m) - 1;
+        const int ibq = __shfl_sync(0xffffffffu, ib, q);
+        if (lane < nc) p.out[((size_t)(blockIdx.x * 32 + q) * p.T + ibq) * p.W + j0 + lane] = t[q][lane];
+      }
+      __syncwarp();
+    }
   }
-  if (lane == 0) p.views[(size_t)s * p.T + ib] = rebin_view_angle(p, s, ib);
+}
+
+// Rows the reference never computes and leaves zero: every row of a slice
+// with start < 0, row 0 of a slice with start == 0 (its raw view would be 0).
+__global__ void __launch_bounds__(256) k_rebin_unvisited(RebinParams p) {
+  const int s = blockIdx.x;
+  const int st = p.start[s];
+  const int nz = st < 0 ? p.T : (st == 0 ? 1 : 0);
+  for (int ib = 0; ib < nz; ++ib) {
+    float* o = p.out + ((size_t)s * p.T + ib) * p.W;
+    for (int j = threadIdx.x; j < p.W; j += blockDim.x) o[j] = 0.f;
+    if (threadIdx.x == 0) p.views[(size_t)s * p.T + ib] = 0.f;
+  }
 }
 
 // Routine layout (after HelicalToFan_routine.m:44-45 permutes, the solver's
@@ -251,13 +289,22 @@ int rebin_prepare(RebinHost& h, long long nViews, const float* zPos, int SLN, fl
   return DDFAN_OK;
 }
 
-int rebin_launch(const RebinParams& p, int layout, cudaStream_t st) {
+// layout 0 (mex layouts): raw-view-order traversal, plus the rows it never
+// visits; layout 1 (slices last): one CTA per (32 slices, view).
+int rebin_launch(const RebinHost& h, int layout, cudaStream_t st) {
+  const RebinParams& p = h.p;
   // 16-byte loads need 16-byte aligned columns: DetHeight % 4 == 0 and an aligned base
   const bool vec = p.H % 4 == 0 && (reinterpret_cast<uintptr_t>(p.raw) & 15) == 0;
   if (layout == 0) {
-    dim3 grid((p.T + kRowsPerCta - 1) / kRowsPerCta, p.SLN);
-    if (vec) k_rebin_mex<true><<<grid, 256, 0, st>>>(p);
-    else k_rebin_mex<false><<<grid, 256, 0, st>>>(p);
+    k_rebin_unvisited<<<p.SLN, 256, 0, st>>>(p);
+    if (h.hi >= h.lo) {
+      const long long nchunk = (h.hi - h.lo + kDiagViews) / kDiagViews;
+      if (nchunk > 65535)
+        return set_err(DDFAN_ERR_UNSUPPORTED, "HelicalToFan: %lld raw views in one call", h.hi - h.lo + 1);
+      dim3 grid((p.SLN + 31) / 32, (unsigned)nchunk);
+      if (vec) k_rebin_diag<true><<<grid, 256, 0, st>>>(p, h.lo, h.hi);
+      else k_rebin_diag<false><<<grid, 256, 0, st>>>(p, h.lo, h.hi);
+    }
   } else {
     dim3 grid(p.T, (p.SLN + 31) / 32);
     if (vec) k_rebin_routine<true><<<grid, 256, 0, st>>>(p);
@@ -314,7 +361,7 @@ extern "C" DDFAN_API int ddfan_helical_to_fan_dev(const float* d_proj, long long
   h.p.view0 = 1;
   h.p.out = d_Proj;
   h.p.views = d_Views;
-  rc = rebin_launch(h.p, layout, st);
+  rc = rebin_launch(h, layout, st);
   dev_free(tables, st);
   return rc;
 }
@@ -355,7 +402,7 @@ extern "C" DDFAN_API int ddfan_HelicalToFan(float* Proj, float* Views, const flo
     h.p.view0 = nraw ? h.lo : 1;
     h.p.out = static_cast<float*>(d_out);
     h.p.views = static_cast<float*>(d_views);
-    rc = rebin_launch(h.p, 0, st);
+    rc = rebin_launch(h, 0, st);
   }
   if (!rc) {
     cudaError_t e = cudaMemcpyAsync(Proj, d_out, out_elems * sizeof(float), cudaMemcpyDeviceToHost, st);

@@ -1,6 +1,7 @@
 // ddfan_solver.cu -- mex-compatible host entry points and the device-resident
 // OS-SART / FISTA solver of libddfan.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -66,36 +67,6 @@ void gather_slab(const float* src, size_t rows, int SLN, int a, int b, std::vect
 void scatter_slab(const std::vector<float>& src, size_t rows, int SLN, int a, int b, float* dst) {
   const int n = b - a;
   for (size_t r = 0; r < rows; ++r) std::memcpy(dst + r * SLN + a, &src[r * n], sizeof(float) * n);
-}
-
-// Distinct angle lists among the slices of hangs[PN][SLN] (bitwise equal
-// columns): slice_list[z] = list of slice z, rep[l] = first slice of list l.
-void angle_lists(const float* hangs, int PN, int SLN, std::vector<int>& slice_list, std::vector<int>& rep) {
-  std::vector<uint64_t> h(SLN, 1469598103934665603ull);
-  for (int q = 0; q < PN; ++q) {
-    const uint32_t* row = reinterpret_cast<const uint32_t*>(hangs + (size_t)q * SLN);
-    for (int z = 0; z < SLN; ++z) h[z] = (h[z] ^ row[z]) * 1099511628211ull;
-  }
-  std::unordered_map<uint64_t, std::vector<int>> by_hash;
-  slice_list.assign(SLN, -1);
-  rep.clear();
-  for (int z = 0; z < SLN; ++z) {
-    std::vector<int>& cand = by_hash[h[z]];
-    for (int l : cand) {
-      bool same = true;
-      for (int q = 0; q < PN && same; ++q)
-        same = std::memcmp(&hangs[(size_t)q * SLN + z], &hangs[(size_t)q * SLN + rep[l]], sizeof(float)) == 0;
-      if (same) {
-        slice_list[z] = l;
-        break;
-      }
-    }
-    if (slice_list[z] < 0) {
-      slice_list[z] = (int)rep.size();
-      cand.push_back((int)rep.size());
-      rep.push_back(z);
-    }
-  }
 }
 
 int device_count() {
@@ -187,35 +158,44 @@ static int mex_call(bool forward, float x0, float y0, int DNU, const float* xds,
 
 // ====================================================================== solver
 
-// Slices [z0, z1) whose angle lists are all list `list`.
-struct Segment {
-  int z0, z1, list;
-};
-
 struct Solver {
-  Plan* P = nullptr;  // SLN slices, PNmax = largest subset
+  Plan* P = nullptr;  // Zi slices, PNmax = largest subset (or largest tile view range)
   int device = 0;
   int PNall = 0, nsub = 1, useFISTA = 1, nonneg = 0, back_mode = DDFAN_BACK_REF;
   int XN = 0, YN = 0, U = 0, Z = 0;
   std::vector<int> off, cnt;  // subset k: rows [off[k], off[k] + cnt[k]) of the subset-ordered tables
-  // Distinct per-slice angle lists (hangs[PNall][SLN] columns): one set of
-  // view tables per list, PNall rows each; runs of consecutive slices with one
-  // list are segments, projected and backprojected by their own launches.
-  int nlists = 1;
-  std::vector<Segment> segs;
-  ViewGeom* d_vg = nullptr;  // [nlists][PNall], subset order
-  double2* d_fc = nullptr;   // [nlists][PNall][U+1]
-  float* d_cvd = nullptr;    // [nlists][PNall][U]
+  ViewGeom* d_vg = nullptr;
+  double2* d_fc = nullptr;
+  float* d_cvd = nullptr;
   int* d_yview = nullptr;  // subset-ordered row -> original view index
-  int* d_order = nullptr;  // [nlists][PNall]: per subset, views in dispatch order (x-major first)
-  int* d_counts = nullptr; // [nlists][nsub][2]: per subset, {x-major views, others}
+  int* d_order = nullptr;  // per subset (or per subset and z-tile): views in dispatch order (x-major first)
+  int* d_counts = nullptr; // per subset: {x-major views, others}
   float* d_rows = nullptr; // [PNall][U]   row sums, subset order
   float* d_cols = nullptr; // [nsub][YN][XN] column sums
-  float* d_y = nullptr;    // [PNall][U][Z] measured sinogram, original order
-  float* d_x = nullptr;
+  float* d_y = nullptr;    // [PNall][U][Zi] measured sinogram
+  float* d_x = nullptr;    // [YN][XN][Zi] image
   float* d_xprev = nullptr;
-  float* d_ax = nullptr;   // [PNmax][U][Z]
+  float* d_ax = nullptr;   // [PNmax][U][Zi]
   double* d_t = nullptr;
+  // Per-slice view angles ("windowed" solver).  Every slice's list is a
+  // window of one table of raw views (view ib of slice z is raw view
+  // off_z + ib): the geometry rows are raw views, grouped by raw view mod
+  // numOfOS (row = (g mod nOS) * Mc + g / nOS).  Internally slices are
+  // reordered so that a z-tile holds slices of one residue off_z mod nOS --
+  // they then need the same raw views for each subset -- and each class is
+  // padded to whole z-tiles; z-tile zt of subset k projects the raw views of
+  // its residue class that fall in its slices' windows.
+  bool win = false;
+  int Zi = 0;                // internal slices (Z when not windowed)
+  int nzt = 0, Mc = 1;
+  std::vector<int> perm;     // internal slice -> original slice, -1 for padding
+  int* d_perm = nullptr;     // the same on the device
+  int* d_inv = nullptr;      // original slice -> internal slice
+  int* d_soff = nullptr;     // internal slice -> window offset (INT_MAX for padding)
+  int4* d_ztd = nullptr;     // [nsub][nzt] view ranges
+  std::vector<int> maxcnt;   // per subset: largest range of a z-tile
+  float* d_xu = nullptr;     // [YN][XN][Z] image in the caller's slice order
+  float* d_stage = nullptr;  // [PNall][U][Z] host sinogram staging (windowed)
   cudaStream_t own = nullptr;
   cudaEvent_t last_use = nullptr;  // recorded after work enqueued on a caller's stream
   cudaGraph_t graph = nullptr;
@@ -238,7 +218,8 @@ static void solver_free(Solver* s) {
   if (s->gexec) cudaGraphExecDestroy(s->gexec);
   if (s->graph) cudaGraphDestroy(s->graph);
   void* ptrs[] = {s->d_vg, s->d_fc, s->d_cvd, s->d_yview, s->d_order, s->d_counts, s->d_rows, s->d_cols,
-                  s->d_y, s->d_x, s->d_xprev, s->d_ax, s->d_t};
+                  s->d_y, s->d_x, s->d_xprev, s->d_ax, s->d_t, s->d_perm, s->d_inv, s->d_soff, s->d_ztd,
+                  s->d_xu, s->d_stage};
   for (void* q : ptrs) dev_free(q, s->own);
   if (s->own) cudaStreamDestroy(s->own);
   if (s->last_use) cudaEventDestroy(s->last_use);
@@ -255,42 +236,67 @@ static int salloc(Solver& s, T** p, size_t n) {
   return rc;
 }
 
+// Slice gathers between the caller's slice order and the internal one:
+// dst[r][t] = map[t] >= 0 ? src[r][map[t]] : 0 for r < rows, t < Zd.
+static __global__ void k_gather_slices(const float* __restrict__ src, int Zs, float* __restrict__ dst, int Zd,
+                                       const int* __restrict__ map, size_t rows) {
+  const size_t n = rows * Zd;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = i / Zd;
+    const int t = (int)(i - r * Zd);
+    const int m = map[t];
+    dst[i] = m >= 0 ? src[r * Zs + m] : 0.f;
+  }
+}
+
+static int gather_slices(const float* src, int Zs, float* dst, int Zd, const int* map, size_t rows,
+                         cudaStream_t st) {
+  const size_t n = rows * Zd;
+  const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+  k_gather_slices<<<std::max(blocks, 1), 256, 0, st>>>(src, Zs, dst, Zd, map, rows);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "slice gather: %s", cudaGetErrorString(e));
+  return DDFAN_OK;
+}
+
 // One OS-SART iteration (AAPM_script/OSSART_AAPM.m:79-115) on stream st.
-// Segments run one after another: slices of a neighbouring segment that share
-// a z-block are computed by each segment's launches but written only by their
-// own, and each segment rebuilds the sinogram table it backprojects.
 static int solver_iteration(Solver& s, cudaStream_t st) {
   Plan& p = *s.P;
   int rc, n = 0;
   const bool adj = s.back_mode == DDFAN_BACK_ADJ;
-  const size_t P = (size_t)s.PNall;
   for (int k = 0; k < s.nsub; ++k) {
     const int o = s.off[k], c = s.cnt[k];
+    BackEpi e{};
+    e.out = s.d_x; e.xin = s.d_x; e.colsum = s.d_cols + (size_t)k * s.XN * s.YN;
+    e.nonneg = s.nonneg; e.mask = p.has_mask ? p.d_mask : nullptr; e.zlo = 0; e.zhi = s.Zi;
     // project the current image (:85)
     if ((rc = launch_sat_image(p, s.d_x, st))) return rc;
-    ++n;
-    for (const Segment& g : s.segs) {
-      const size_t r = (size_t)g.list * P + o;
-      const ViewGeom* vg = s.d_vg + r;
-      const double2* fc = s.d_fc + r * (s.U + 1);
-      const float* cvd = s.d_cvd + r * s.U;
-      const int* order = s.d_order + r;
-      if ((rc = launch_fwd(p, vg, fc, cvd, order, c, s.d_ax, g.z0, g.z1, st))) return rc;
+    if (!s.win) {
+      const ViewGeom* vg = s.d_vg + o;
+      const double2* fc = s.d_fc + (size_t)o * (s.U + 1);
+      const float* cvd = s.d_cvd + (size_t)o * s.U;
+      if ((rc = launch_fwd(p, vg, fc, cvd, s.d_order + o, c, s.d_ax, 0, s.Zi, st))) return rc;
       // residual (y - A x) / rowSum folded into the sinogram prefix sums (:86-88)
       if ((rc = launch_sat_sino(p, s.d_ax, c, adj ? cvd : nullptr, 1.f, s.d_y, s.d_yview + o,
-                                s.d_rows + (size_t)o * s.U, st, g.z0, g.z1)))
+                                s.d_rows + (size_t)o * s.U, st)))
         return rc;
       // backproject, divide by colSum, add, optional clamp (:91-97)
-      BackEpi e{};
-      e.out = s.d_x; e.xin = s.d_x; e.colsum = s.d_cols + (size_t)k * s.XN * s.YN;
-      e.nonneg = s.nonneg; e.mask = p.has_mask ? p.d_mask : nullptr; e.zlo = g.z0; e.zhi = g.z1;
-      const int* counts = s.d_counts + ((size_t)g.list * s.nsub + k) * 2;
-      if ((rc = launch_back(p, s.back_mode, vg, fc, order, counts, c, e, st))) return rc;
-      n += adj ? 4 : 3;
+      if ((rc = launch_back(p, s.back_mode, vg, fc, s.d_order + o, s.d_counts + 2 * k, c, e, st))) return rc;
+    } else {
+      const int4* ztd = s.d_ztd + (size_t)k * s.nzt;
+      const int m = s.maxcnt[k];
+      ViewRanges vr;
+      vr.ztd = ztd; vr.soff = s.d_soff; vr.Mc = s.Mc; vr.nOS = s.nsub; vr.ksub = k; vr.T = s.PNall;
+      if ((rc = launch_fwd(p, s.d_vg, s.d_fc, s.d_cvd, s.d_order, m, s.d_ax, 0, s.Zi, st, ztd))) return rc;
+      if ((rc = launch_sat_sino(p, s.d_ax, m, adj ? s.d_cvd : nullptr, 1.f, s.d_y, nullptr,
+                                s.d_rows + (size_t)o * s.U, st, 0, s.Zi, &vr)))
+        return rc;
+      if ((rc = launch_back(p, s.back_mode, s.d_vg, s.d_fc, s.d_order, nullptr, m, e, st, ztd))) return rc;
     }
+    n += adj ? 5 : 4;
   }
   if (s.useFISTA) {
-    const size_t V = (size_t)s.XN * s.YN * s.Z;
+    const size_t V = (size_t)s.XN * s.YN * s.Zi;
     const int blocks = (int)std::min<size_t>((V + 255) / 256, 148 * 16);
     ProfScope ps(KIND_FISTA, st);
     k_fista<<<blocks, 256, 0, st>>>(s.d_x, s.d_xprev, V, s.d_t);
@@ -300,6 +306,169 @@ static int solver_iteration(Solver& s, cudaStream_t st) {
     n += 2;
   }
   s.launches = n;
+  return DDFAN_OK;
+}
+
+// The image in the caller's slice order (windowed solver), after iterations.
+static int solver_publish(Solver& s, cudaStream_t st) {
+  if (!s.win) return DDFAN_OK;
+  return gather_slices(s.d_x, s.Zi, s.d_xu, s.Z, s.d_inv, (size_t)s.XN * s.YN, st);
+}
+
+// Every slice's angle list as a window of one raw-view table: view ib of
+// slice z is G[off[z] + ib], bitwise.  A slice continues the table where its
+// list overlaps the previous slice's window end (helical rebinning: slice z+1
+// starts a few raw views after slice z), reuses an identical earlier window,
+// or appends its whole list.
+static void angle_windows(const float* hangs, int T, int SLN, std::vector<float>& G, std::vector<int>& off) {
+  G.clear();
+  off.assign(SLN, 0);
+  auto bits = [](float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; };
+  auto at = [&](int ib, int z) { return bits(hangs[(size_t)ib * SLN + z]); };
+  std::unordered_map<uint64_t, std::vector<int>> seen;  // list hash -> slices with that window
+  for (int z = 0; z < SLN; ++z) {
+    uint64_t h = 1469598103934665603ull;
+    for (int ib = 0; ib < T; ++ib) h = (h ^ at(ib, z)) * 1099511628211ull;
+    int placed = -1;
+    if (z > 0 && (size_t)off[z - 1] + T == G.size()) {
+      const int base = off[z - 1];
+      const uint32_t first = at(0, z);
+      for (int d = 0; d < T && placed < 0; ++d) {
+        if (bits(G[base + d]) != first) continue;
+        bool ok = true;
+        for (int ib = 0; ib < T - d && ok; ++ib) ok = at(ib, z) == bits(G[base + d + ib]);
+        if (ok) {
+          placed = base + d;
+          for (int ib = T - d; ib < T; ++ib) G.push_back(hangs[(size_t)ib * SLN + z]);
+        }
+      }
+    }
+    if (placed < 0) {
+      for (int y : seen[h]) {
+        bool ok = true;
+        for (int ib = 0; ib < T && ok; ++ib) ok = at(ib, z) == at(ib, y);
+        if (ok) {
+          placed = off[y];
+          break;
+        }
+      }
+    }
+    if (placed < 0) {
+      placed = (int)G.size();
+      for (int ib = 0; ib < T; ++ib) G.push_back(hangs[(size_t)ib * SLN + z]);
+    }
+    off[z] = placed;
+    seen[h].push_back(z);
+  }
+}
+
+// Internal slice order, z-tile width and view ranges of the windowed solver.
+struct WinLayout {
+  int ZL = 1, Zi = 0, nzt = 0, Mc = 1, PNmax = 0;
+  std::vector<int> perm, soff;
+  std::vector<int4> ztd;  // [nsub][nzt], .w filled on the device
+  std::vector<int> maxcnt;
+  long long cost = 0;
+};
+
+static void win_layout(const std::vector<int>& off, int NG, int T, int nOS, int ZL, WinLayout& w) {
+  const int SLN = (int)off.size();
+  w.ZL = ZL;
+  w.Mc = (NG + nOS - 1) / nOS + 1;
+  std::vector<int> idx(SLN);
+  for (int z = 0; z < SLN; ++z) idx[z] = z;
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+    const int ra = off[a] % nOS, rb = off[b] % nOS;
+    return ra != rb ? ra < rb : off[a] < off[b];
+  });
+  const int tile = 4 * ZL;
+  w.perm.clear();
+  for (size_t i = 0; i < idx.size();) {
+    size_t j = i;
+    const int r = off[idx[i]] % nOS;
+    while (j < idx.size() && off[idx[j]] % nOS == r) w.perm.push_back(idx[j++]);
+    while (w.perm.size() % tile) w.perm.push_back(-1);
+    i = j;
+  }
+  w.Zi = (int)w.perm.size();
+  w.nzt = w.Zi / tile;
+  w.soff.assign(w.Zi, INT_MAX);
+  for (int t = 0; t < w.Zi; ++t)
+    if (w.perm[t] >= 0) w.soff[t] = off[w.perm[t]];
+  w.ztd.assign((size_t)nOS * w.nzt, make_int4(0, 0, 0, 0));
+  w.maxcnt.assign(nOS, 0);
+  w.PNmax = 0;
+  w.cost = 0;
+  int ooff = 0;
+  for (int k = 0; k < nOS; ++k) {
+    for (int zt = 0; zt < w.nzt; ++zt) {
+      int lo = INT_MAX, hi = INT_MIN, r = 0;
+      for (int t = zt * tile; t < (zt + 1) * tile; ++t)
+        if (w.perm[t] >= 0) {
+          lo = std::min(lo, w.soff[t]);
+          hi = std::max(hi, w.soff[t] + T - 1);
+          r = w.soff[t] % nOS;
+        }
+      const int c = (r + k) % nOS;
+      // raw views g = c (mod nOS) in [lo, hi]
+      const int gf = lo + ((c - lo % nOS) % nOS + nOS) % nOS;
+      const int count = gf > hi ? 0 : (hi - gf) / nOS + 1;
+      w.ztd[(size_t)k * w.nzt + zt] = make_int4(c * w.Mc + (gf - c) / nOS, count, ooff, 0);
+      ooff += count;
+      w.maxcnt[k] = std::max(w.maxcnt[k], count);
+      w.PNmax = std::max(w.PNmax, count);
+      w.cost += (long long)count;
+    }
+  }
+}
+
+// Row sums and column sums of every subset from slice 0's angles, on a
+// one-slice plan (AAPM_script/OSSART_AAPM.m:57-66).
+static int solver_weights(Solver& s, const PlanDesc& d, const std::vector<float>& angs0, int PNmax, cudaStream_t st) {
+  const int XN = s.XN, YN = s.YN, DNU = s.U, P = s.PNall;
+  PlanDesc d1 = d;
+  d1.SLN = 1;
+  d1.PNmax = PNmax;
+  d1.zl_force = 0;
+  PlanPtr P1;
+  int rc = plan_create(&P1.p, d1);
+  if (rc) return rc;
+  DevBuf<ViewGeom> vg(st);
+  DevBuf<double2> fc(st);
+  DevBuf<float> cvd(st), ang(st), ones(st);
+  DevBuf<int> order(st), counts(st);
+  const size_t n1 = std::max((size_t)XN * YN, (size_t)PNmax * DNU);
+  if ((rc = vg.alloc(P)) || (rc = fc.alloc((size_t)P * (DNU + 1))) || (rc = cvd.alloc((size_t)P * DNU)) ||
+      (rc = ang.alloc(P)) || (rc = ones.alloc(n1)) || (rc = order.alloc(P)) || (rc = counts.alloc(2 * (size_t)s.nsub)))
+    return rc;
+  std::vector<float> h1(n1, 1.0f);
+  DDFAN_CK(cudaMemcpyAsync(ones.p, h1.data(), sizeof(float) * n1, cudaMemcpyHostToDevice, st));
+  DDFAN_CK(cudaMemcpyAsync(ang.p, angs0.data(), sizeof(float) * P, cudaMemcpyHostToDevice, st));
+  if ((rc = launch_view_geom(*P1.p, ang.p, 1, P, vg.p, fc.p, cvd.p, st))) return rc;
+  for (int k = 0; k < s.nsub; ++k)
+    if ((rc = launch_view_order(vg.p + s.off[k], s.cnt[k], order.p + s.off[k], counts.p + 2 * k, st))) return rc;
+  if ((rc = launch_sat_image(*P1.p, ones.p, st))) return rc;
+  for (int k = 0; k < s.nsub; ++k) {
+    const int o = s.off[k], c = s.cnt[k];
+    if ((rc = launch_fwd(*P1.p, vg.p + o, fc.p + (size_t)o * (DNU + 1), cvd.p + (size_t)o * DNU, order.p + o, c,
+                         s.d_rows + (size_t)o * DNU, 0, 1, st)))
+      return rc;
+  }
+  const bool adj = s.back_mode == DDFAN_BACK_ADJ;
+  for (int k = 0; k < s.nsub; ++k) {
+    const int o = s.off[k], c = s.cnt[k];
+    if ((rc = launch_sat_sino(*P1.p, ones.p, c, adj ? cvd.p + (size_t)o * DNU : nullptr, 1.f, nullptr, nullptr,
+                              nullptr, st)))
+      return rc;
+    BackEpi e{};
+    e.out = s.d_cols + (size_t)k * XN * YN;
+    e.mask = P1.p->has_mask ? P1.p->d_mask : nullptr;
+    e.zlo = 0; e.zhi = 1;
+    if ((rc = launch_back(*P1.p, s.back_mode, vg.p + o, fc.p + (size_t)o * (DNU + 1), order.p + o,
+                          counts.p + 2 * k, c, e, st)))
+      return rc;
+  }
+  DDFAN_CK(cudaStreamSynchronize(st));
   return DDFAN_OK;
 }
 
@@ -318,107 +487,111 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
   Solver& s = *S;
   s.device = device; s.PNall = PNall; s.nsub = numOfOS; s.useFISTA = useFISTA ? 1 : 0;
   s.nonneg = nonneg ? 1 : 0; s.back_mode = back_mode; s.XN = XN; s.YN = YN; s.U = DNU; s.Z = SLN;
-  // distinct angle lists (bitwise) and the slices' runs of them
-  std::vector<int> rep, slice_list(SLN);
-  angle_lists(hangs, PNall, SLN, slice_list, rep);
-  s.nlists = (int)rep.size();
-  int shortest = SLN;
-  for (int z = 0; z < SLN;) {
-    int e = z + 1;
-    while (e < SLN && slice_list[e] == slice_list[z]) ++e;
-    s.segs.push_back({z, e, slice_list[z]});
-    shortest = std::min(shortest, e - z);
-    z = e;
-  }
   // subsets k, k + numOfOS, ... (AAPM_script/OSSART_AAPM.m:60)
   std::vector<int> yview;
-  int PNmax = 0;
+  int PNsub = 0;
   for (int k = 0; k < numOfOS; ++k) {
     s.off.push_back((int)yview.size());
     for (int v = k; v < PNall; v += numOfOS) yview.push_back(v);
     s.cnt.push_back((int)yview.size() - s.off.back());
-    PNmax = std::max(PNmax, s.cnt.back());
+    PNsub = std::max(PNsub, s.cnt.back());
   }
-  const size_t P = (size_t)PNall, L = (size_t)s.nlists;
-  std::vector<float> angs(L * P);
-  for (size_t l = 0; l < L; ++l)
-    for (size_t r = 0; r < P; ++r) angs[l * P + r] = hangs[(size_t)yview[r] * SLN + rep[l]];
-  PlanDesc d{x0, y0, DNU, xds, yds, detCntIdx, imgXCenter, imgYCenter, XN, YN, dx, mask, SLN, PNmax,
+  const size_t P = (size_t)PNall;
+  std::vector<float> angs0(P);  // slice 0's angles, subset order
+  for (size_t r = 0; r < P; ++r) angs0[r] = hangs[(size_t)yview[r] * SLN];
+  // per-slice angle lists as windows of one raw-view table
+  std::vector<float> G;
+  std::vector<int> woff;
+  angle_windows(hangs, PNall, SLN, G, woff);
+  s.win = false;
+  for (int z = 1; z < SLN; ++z) s.win = s.win || woff[z] != woff[0];
+  WinLayout W;
+  if (s.win) {
+    // z-tile width: views per tile x blocks per tile x relative cost of a block
+    // at that width (the projector cost model of pow2_zl)
+    const int widths[4] = {1, 2, 4, 8};
+    const double unit[4] = {3.6, 2.1, 1.2, 1.0};
+    double best = -1;
+    for (int i = 0; i < 4; ++i) {
+      WinLayout t;
+      win_layout(woff, (int)G.size(), PNall, numOfOS, widths[i], t);
+      const double c = (double)t.cost * widths[i] * unit[i];
+      if (best < 0 || c < best) {
+        best = c;
+        W = t;
+      }
+    }
+    if (W.PNmax > 65535) return set_err(DDFAN_ERR_UNSUPPORTED, "solver: %d views in one z-tile range", W.PNmax);
+    s.Zi = W.Zi; s.nzt = W.nzt; s.Mc = W.Mc; s.perm = W.perm; s.maxcnt = W.maxcnt;
+  } else {
+    s.Zi = SLN;
+  }
+  const int PNmax = s.win ? W.PNmax : PNsub;
+  PlanDesc d{x0, y0, DNU, xds, yds, detCntIdx, imgXCenter, imgYCenter, XN, YN, dx, mask, s.Zi, std::max(PNmax, 1),
              sat_mode, device};
-  // z-tiles no wider than the shortest segment (a launch computes whole tiles)
-  if (s.segs.size() > 1) d.zl_cap = std::max(1, std::min(8, shortest / 4));
+  if (s.win) d.zl_force = W.ZL;
   int rc = plan_create(&s.P, d);
   if (rc) return rc;
   s.bytes = s.P->bytes;
   DeviceGuard g(device);
-  const size_t V = (size_t)XN * YN * SLN;
+  const size_t V = (size_t)XN * YN * s.Zi;
+  const size_t R = s.win ? (size_t)numOfOS * s.Mc : P;  // geometry rows
+  const size_t nord = s.win ? (size_t)std::max<long long>(W.cost, 1) : P;
   DDFAN_CK(cudaStreamCreateWithFlags(&s.own, cudaStreamNonBlocking));
   DDFAN_CK(cudaEventCreateWithFlags(&s.last_use, cudaEventDisableTiming));
-  if ((rc = salloc(s, &s.d_vg, L * P)) || (rc = salloc(s, &s.d_fc, L * P * (DNU + 1))) ||
-      (rc = salloc(s, &s.d_cvd, L * P * DNU)) || (rc = salloc(s, &s.d_yview, PNall)) ||
-      (rc = salloc(s, &s.d_order, L * P)) || (rc = salloc(s, &s.d_counts, L * 2 * (size_t)numOfOS)) ||
-      (rc = salloc(s, &s.d_rows, (size_t)PNall * DNU)) ||
-      (rc = salloc(s, &s.d_cols, (size_t)numOfOS * XN * YN)) ||
-      (rc = salloc(s, &s.d_y, (size_t)PNall * DNU * SLN)) || (rc = salloc(s, &s.d_x, V)) ||
-      (rc = salloc(s, &s.d_xprev, V)) || (rc = salloc(s, &s.d_ax, (size_t)PNmax * DNU * SLN)) ||
-      (rc = salloc(s, &s.d_t, 1)))
+  if ((rc = salloc(s, &s.d_vg, R)) || (rc = salloc(s, &s.d_fc, R * (DNU + 1))) ||
+      (rc = salloc(s, &s.d_cvd, R * DNU)) || (rc = salloc(s, &s.d_yview, P)) || (rc = salloc(s, &s.d_order, nord)) ||
+      (rc = salloc(s, &s.d_counts, 2 * (size_t)numOfOS)) || (rc = salloc(s, &s.d_rows, P * DNU)) ||
+      (rc = salloc(s, &s.d_cols, (size_t)numOfOS * XN * YN)) || (rc = salloc(s, &s.d_y, P * DNU * s.Zi)) ||
+      (rc = salloc(s, &s.d_x, V)) || (rc = salloc(s, &s.d_xprev, V)) ||
+      (rc = salloc(s, &s.d_ax, (size_t)std::max(PNmax, 1) * DNU * s.Zi)) || (rc = salloc(s, &s.d_t, 1)))
     return rc;
   cudaStream_t st = s.own;
-  // per-view tables for every view of every list, in subset order
-  DevBuf<float> dang(st);
-  if ((rc = dang.alloc(L * P))) return rc;
-  DDFAN_CK(cudaMemcpyAsync(dang.p, angs.data(), sizeof(float) * L * P, cudaMemcpyHostToDevice, st));
-  DDFAN_CK(cudaMemcpyAsync(s.d_yview, yview.data(), sizeof(int) * PNall, cudaMemcpyHostToDevice, st));
-  if ((rc = launch_view_geom(*s.P, dang.p, 1, (int)(L * P), s.d_vg, s.d_fc, s.d_cvd, st))) return rc;
-  // per list and subset: views of one orientation together (one image table
-  // at a time stays hot in L2; the exact adjoint visits each orientation in turn)
-  for (size_t l = 0; l < L; ++l)
+  DDFAN_CK(cudaMemcpyAsync(s.d_yview, yview.data(), sizeof(int) * P, cudaMemcpyHostToDevice, st));
+  if (!s.win) {
+    // per-view tables for every view, in subset order; per subset the views
+    // of one orientation together (one image table at a time stays hot in
+    // L2; the exact adjoint visits each orientation in turn)
+    DevBuf<float> dang(st);
+    if ((rc = dang.alloc(P))) return rc;
+    DDFAN_CK(cudaMemcpyAsync(dang.p, angs0.data(), sizeof(float) * P, cudaMemcpyHostToDevice, st));
+    if ((rc = launch_view_geom(*s.P, dang.p, 1, PNall, s.d_vg, s.d_fc, s.d_cvd, st))) return rc;
     for (int k = 0; k < numOfOS; ++k)
-      if ((rc = launch_view_order(s.d_vg + l * P + s.off[k], s.cnt[k], s.d_order + l * P + s.off[k],
-                                  s.d_counts + (l * numOfOS + k) * 2, st)))
+      if ((rc = launch_view_order(s.d_vg + s.off[k], s.cnt[k], s.d_order + s.off[k], s.d_counts + 2 * k, st)))
         return rc;
-  // the weights use slice 0's angles (AAPM_script/OSSART_AAPM.m:61-64)
-  const size_t l0 = (size_t)slice_list[0] * P;
-  // row / column sums from slice 0 on a one-slice plan (AAPM_script/OSSART_AAPM.m:59-66)
-  {
-    PlanDesc d1 = d;
-    d1.SLN = 1;
-    PlanPtr P1;
-    if ((rc = plan_create(&P1.p, d1))) return rc;
-    DevBuf<float> ones(st), tmp(st);
-    const size_t n1 = std::max((size_t)XN * YN, (size_t)PNmax * DNU);
-    if ((rc = ones.alloc(n1)) || (rc = tmp.alloc((size_t)PNmax * DNU))) return rc;
-    std::vector<float> h1(n1, 1.0f);
-    DDFAN_CK(cudaMemcpyAsync(ones.p, h1.data(), sizeof(float) * n1, cudaMemcpyHostToDevice, st));
-    if ((rc = launch_sat_image(*P1.p, ones.p, st))) return rc;
-    for (int k = 0; k < numOfOS; ++k) {
-      const size_t o = l0 + s.off[k];
-      const int c = s.cnt[k];
-      if ((rc = launch_fwd(*P1.p, s.d_vg + o, s.d_fc + o * (DNU + 1), s.d_cvd + o * DNU, s.d_order + o, c,
-                           s.d_rows + (size_t)s.off[k] * DNU, 0, 1, st)))
-        return rc;
+    DDFAN_CK(cudaStreamSynchronize(st));
+  } else {
+    // raw-view geometry rows, grouped by residue; per (subset, z-tile) range
+    // the slot order (x-major first) and its x-major count
+    std::vector<float> rows(R, 0.f), soff_h(W.soff.begin(), W.soff.end());
+    for (size_t r = 0; r < R; ++r) {
+      const size_t gv = r / s.Mc + (r % s.Mc) * (size_t)numOfOS;
+      if (gv < G.size()) rows[r] = G[gv];
     }
-    for (int k = 0; k < numOfOS; ++k) {
-      const size_t o = l0 + s.off[k];
-      const int c = s.cnt[k];
-      const bool adj = back_mode == DDFAN_BACK_ADJ;
-      if ((rc = launch_sat_sino(*P1.p, ones.p, c, adj ? s.d_cvd + o * DNU : nullptr, 1.f, nullptr, nullptr,
-                                nullptr, st)))
-        return rc;
-      BackEpi e{};
-      e.out = s.d_cols + (size_t)k * XN * YN;
-      e.mask = P1.p->has_mask ? P1.p->d_mask : nullptr;
-      e.zlo = 0; e.zhi = 1;
-      if ((rc = launch_back(*P1.p, back_mode, s.d_vg + o, s.d_fc + o * (DNU + 1), s.d_order + o,
-                            s.d_counts + ((size_t)slice_list[0] * numOfOS + k) * 2, c, e, st)))
-        return rc;
-    }
+    std::vector<int> inv(SLN, 0);
+    for (int t = 0; t < s.Zi; ++t)
+      if (s.perm[t] >= 0) inv[s.perm[t]] = t;
+    DevBuf<float> dang(st);
+    if ((rc = dang.alloc(R)) || (rc = salloc(s, &s.d_perm, s.Zi)) || (rc = salloc(s, &s.d_inv, SLN)) ||
+        (rc = salloc(s, &s.d_soff, s.Zi)) || (rc = salloc(s, &s.d_ztd, W.ztd.size())) ||
+        (rc = salloc(s, &s.d_xu, (size_t)XN * YN * SLN)) || (rc = salloc(s, &s.d_stage, P * DNU * SLN)))
+      return rc;
+    DDFAN_CK(cudaMemcpyAsync(dang.p, rows.data(), sizeof(float) * R, cudaMemcpyHostToDevice, st));
+    DDFAN_CK(cudaMemcpyAsync(s.d_perm, s.perm.data(), sizeof(int) * s.Zi, cudaMemcpyHostToDevice, st));
+    DDFAN_CK(cudaMemcpyAsync(s.d_inv, inv.data(), sizeof(int) * SLN, cudaMemcpyHostToDevice, st));
+    DDFAN_CK(cudaMemcpyAsync(s.d_soff, W.soff.data(), sizeof(int) * s.Zi, cudaMemcpyHostToDevice, st));
+    DDFAN_CK(cudaMemcpyAsync(s.d_ztd, W.ztd.data(), sizeof(int4) * W.ztd.size(), cudaMemcpyHostToDevice, st));
+    if ((rc = launch_view_geom(*s.P, dang.p, 1, (int)R, s.d_vg, s.d_fc, s.d_cvd, st))) return rc;
+    if ((rc = launch_view_order_ranges(s.d_vg, s.d_ztd, (int)W.ztd.size(), s.d_order, st))) return rc;
+    DDFAN_CK(cudaMemsetAsync(s.d_xu, 0, sizeof(float) * XN * YN * SLN, st));
     DDFAN_CK(cudaStreamSynchronize(st));
   }
+  if ((rc = solver_weights(s, d, angs0, PNsub, st))) return rc;
   const double one = 1.0;
   DDFAN_CK(cudaMemcpyAsync(s.d_t, &one, sizeof(double), cudaMemcpyHostToDevice, st));
   DDFAN_CK(cudaMemsetAsync(s.d_x, 0, sizeof(float) * V, st));
   DDFAN_CK(cudaMemsetAsync(s.d_xprev, 0, sizeof(float) * V, st));
+  DDFAN_CK(cudaMemsetAsync(s.d_y, 0, sizeof(float) * P * DNU * s.Zi, st));
   DDFAN_CK(cudaStreamSynchronize(st));
   *out = S.release();
   return DDFAN_OK;
@@ -492,10 +665,21 @@ DDFAN_API int ddfan_ossart_set_sinogram(ddfan_ossart* h, const float* proj, int 
   if (!s || !proj) return set_err(DDFAN_ERR_ARG, "null argument");
   DeviceGuard g(s->device);
   const size_t n = (size_t)s->PNall * s->U * s->Z;
-  DDFAN_CK(cudaMemcpyAsync(s->d_y, proj, sizeof(float) * n,
-                           is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                           (cudaStream_t)stream));
-  cudaEventRecord(s->last_use, (cudaStream_t)stream);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!s->win) {
+    DDFAN_CK(cudaMemcpyAsync(s->d_y, proj, sizeof(float) * n,
+                             is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+  } else {
+    // into the internal slice order
+    const float* src = proj;
+    if (!is_device) {
+      DDFAN_CK(cudaMemcpyAsync(s->d_stage, proj, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+      src = s->d_stage;
+    }
+    int rc = gather_slices(src, s->Z, s->d_y, s->Zi, s->d_perm, (size_t)s->PNall * s->U, st);
+    if (rc) return rc;
+  }
+  cudaEventRecord(s->last_use, st);
   return DDFAN_OK;
 }
 
@@ -505,9 +689,17 @@ DDFAN_API int ddfan_ossart_set_image(ddfan_ossart* h, const float* img, int is_d
   DeviceGuard g(s->device);
   const size_t n = (size_t)s->XN * s->YN * s->Z;
   cudaStream_t st = (cudaStream_t)stream;
-  DDFAN_CK(cudaMemcpyAsync(s->d_x, img, sizeof(float) * n,
-                           is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
-  DDFAN_CK(cudaMemcpyAsync(s->d_xprev, s->d_x, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+  if (!s->win) {
+    DDFAN_CK(cudaMemcpyAsync(s->d_x, img, sizeof(float) * n,
+                             is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+  } else {
+    DDFAN_CK(cudaMemcpyAsync(s->d_xu, img, sizeof(float) * n,
+                             is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    int rc = gather_slices(s->d_xu, s->Z, s->d_x, s->Zi, s->d_perm, (size_t)s->XN * s->YN, st);
+    if (rc) return rc;
+  }
+  DDFAN_CK(cudaMemcpyAsync(s->d_xprev, s->d_x, sizeof(float) * (size_t)s->XN * s->YN * s->Zi,
+                           cudaMemcpyDeviceToDevice, st));
   static const double one = 1.0;
   DDFAN_CK(cudaMemcpyAsync(s->d_t, &one, sizeof(double), cudaMemcpyHostToDevice, st));
   // the pageable host sources above must be consumed before returning
@@ -525,6 +717,8 @@ DDFAN_API int ddfan_ossart_iterate(ddfan_ossart* h, int numOfIter, int use_graph
       int rc = solver_iteration(*s, st);
       if (rc) return rc;
     }
+    int rc = solver_publish(*s, st);
+    if (rc) return rc;
     cudaEventRecord(s->last_use, st);
     return DDFAN_OK;
   }
@@ -542,6 +736,8 @@ DDFAN_API int ddfan_ossart_iterate(ddfan_ossart* h, int numOfIter, int use_graph
     DDFAN_CK(cudaGraphInstantiate(&s->gexec, s->graph, 0));
   }
   for (int it = 0; it < numOfIter; ++it) DDFAN_CK(cudaGraphLaunch(s->gexec, st));
+  int rc = solver_publish(*s, st);
+  if (rc) return rc;
   cudaEventRecord(s->last_use, st);
   return DDFAN_OK;
 }
@@ -552,7 +748,7 @@ DDFAN_API int ddfan_ossart_get_image(ddfan_ossart* h, float* img, int is_device,
   DeviceGuard g(s->device);
   const size_t n = (size_t)s->XN * s->YN * s->Z;
   cudaStream_t st = (cudaStream_t)stream;
-  DDFAN_CK(cudaMemcpyAsync(img, s->d_x, sizeof(float) * n,
+  DDFAN_CK(cudaMemcpyAsync(img, s->win ? s->d_xu : s->d_x, sizeof(float) * n,
                            is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
   cudaEventRecord(s->last_use, st);
   if (!is_device) DDFAN_CK(cudaStreamSynchronize(st));
@@ -587,14 +783,13 @@ DDFAN_API int ddfan_ossart_profile(ddfan_ossart* h, int numOfIter, void* stream,
 
 DDFAN_API float* ddfan_ossart_image_ptr(ddfan_ossart* h) {
   Solver* s = reinterpret_cast<Solver*>(h);
-  return s ? s->d_x : nullptr;
+  return s ? (s->win ? s->d_xu : s->d_x) : nullptr;
 }
 
 DDFAN_API int ddfan_ossart_launches_per_iter(const ddfan_ossart* h) {
   const Solver* s = reinterpret_cast<const Solver*>(h);
   if (!s) return 0;
-  const int per_seg = s->back_mode == DDFAN_BACK_ADJ ? 4 : 3;
-  return s->nsub * (1 + (int)s->segs.size() * per_seg) + (s->useFISTA ? 2 : 0);
+  return s->nsub * (s->back_mode == DDFAN_BACK_ADJ ? 5 : 4) + (s->useFISTA ? 2 : 0);
 }
 
 DDFAN_API int ddfan_OSSART_AAPM(float x0, float y0, int DNU, const float* xds, const float* yds,

@@ -217,7 +217,7 @@ def rebinned_angles(PN, SLN, starts, BV=0.3):
 
 
 @pytest.mark.parametrize("back", ["ref", "adj"])
-@pytest.mark.parametrize("lists", ["rebinned", "repeating"])
+@pytest.mark.parametrize("lists", ["rebinned", "repeating", "unrelated"])
 def test_ossart_per_slice_angles_matches_oracle(mods, back, lists):
     """OSSART_AAPM with Views(SLN, PN) that differ per slice (the rebinned
     real-data case): every slice is projected with its own angles and the
@@ -229,10 +229,14 @@ def test_ossart_per_slice_angles_matches_oracle(mods, back, lists):
     x0, y0, xds, yds = dd2.fan_geometry(s.sid, s.sdd, s.DNU, s.detCellWidth, s.detCntIdx)
     if lists == "rebinned":
         h = rebinned_angles(s.PN, SLN, [37 * z + 5 for z in range(SLN)])
-    else:
-        # three lists over seven slices: segments A A | B | C | A | C C
+    elif lists == "repeating":
+        # three lists over seven slices: A A B C A C C
         base = rebinned_angles(s.PN, 3, [0, 11, 50])
         h = base[:, [0, 0, 1, 2, 0, 2, 2]].copy()
+    else:
+        # no slice's list is a shifted window of another's
+        rng = np.random.default_rng(3)
+        h = (s.hangs() + rng.uniform(0, 2 * math.pi, SLN)[None, :].astype(np.float32)).astype(np.float32)
     xt = configs.phantom(s)
     mask = s.circular_mask()
     y = O.proj(x0, y0, s.DNU, xds, yds, 0, 0, h, s.PN, s.XN, s.YN, SLN, xt, s.dx, mask)
