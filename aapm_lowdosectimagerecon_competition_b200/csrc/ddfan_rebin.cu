@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -316,20 +317,55 @@ int rebin_launch(const RebinHost& h, int layout, cudaStream_t st) {
 }
 
 // small host->device uploads of the per-channel and per-slice tables into one buffer
+// Pinned staging for the small per-call tables, one per device: a pageable
+// source would make cudaMemcpyAsync wait for the stream, leaving the GPU idle
+// between back-to-back calls.  The buffer is reused once the previous call's
+// copy out of it has completed (its event), so a call never waits for kernels.
+struct Staging {
+  std::mutex m;
+  unsigned char* host = nullptr;
+  size_t cap = 0;
+  cudaEvent_t copied = nullptr;
+};
+constexpr int kMaxStagingDevices = 64;
+Staging g_staging[kMaxStagingDevices];
+
 int rebin_tables(RebinHost& h, const float* zPos, void** buf, cudaStream_t st) {
   const int W = h.p.W, SLN = h.p.SLN;
   const size_t b_sm = ((sizeof(float) * W + 255) / 256) * 256;
   const size_t b_z = ((sizeof(float) * SLN + 255) / 256) * 256;
   const size_t bytes = b_sm + b_z + sizeof(int) * SLN;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxStagingDevices) {
+    cudaGetLastError();
+    return set_err(DDFAN_ERR_CUDA, "HelicalToFan: no usable current device");
+  }
   int rc = dev_alloc(buf, bytes, st);
   if (rc) return rc;
   unsigned char* b = static_cast<unsigned char*>(*buf);
-  cudaError_t e = cudaMemcpyAsync(b, h.sm.data(), sizeof(float) * W, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(b + b_sm, zPos, sizeof(float) * SLN, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(b + b_sm + b_z, h.start.data(), sizeof(int) * SLN, cudaMemcpyHostToDevice, st);
+  Staging& sg = g_staging[dev];
+  std::lock_guard<std::mutex> lock(sg.m);
+  cudaError_t e = cudaSuccess;
+  if (!sg.copied) e = cudaEventCreateWithFlags(&sg.copied, cudaEventDisableTiming);
+  else e = cudaEventSynchronize(sg.copied);  // the previous upload has left the buffer
+  if (e == cudaSuccess && sg.cap < bytes) {
+    if (sg.host) cudaFreeHost(sg.host);
+    sg.host = nullptr;
+    sg.cap = 0;
+    e = cudaHostAlloc(reinterpret_cast<void**>(&sg.host), bytes, cudaHostAllocDefault);
+    if (e == cudaSuccess) sg.cap = bytes;
+  }
+  if (e == cudaSuccess) {
+    std::memcpy(sg.host, h.sm.data(), sizeof(float) * W);
+    std::memcpy(sg.host + b_sm, zPos, sizeof(float) * SLN);
+    std::memcpy(sg.host + b_sm + b_z, h.start.data(), sizeof(int) * SLN);
+    e = cudaMemcpyAsync(b, sg.host, bytes, cudaMemcpyHostToDevice, st);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(sg.copied, st);
   if (e != cudaSuccess) {
     cudaGetLastError();
+    dev_free(*buf, st);
+    *buf = nullptr;
     return set_err(DDFAN_ERR_CUDA, "HelicalToFan table upload: %s", cudaGetErrorString(e));
   }
   h.p.sm = reinterpret_cast<const float*>(b);

@@ -308,7 +308,7 @@ def run_rebin(args):
     achieved = alg / (ms_per_step / 1e3) / 1e9
     traffic = None
     try:
-        with open(os.path.join(ROOT, "profiles", "k_rebin_routine.md")) as fh:
+        with open(os.path.join(ROOT, "profiles", "k_rebin_routine_siemens512.md")) as fh:
             for ln in fh:
                 if ln.startswith("traffic_bytes_per_launch:"):
                     traffic = float(ln.split(":", 1)[1])
@@ -327,7 +327,7 @@ def run_rebin(args):
         proj_h = d_raw.cpu().numpy()
     if not args.no_e2e:
         t_e2e = []
-        for rep in range(2):
+        for rep in range(3):
             torch.cuda.synchronize(dev)
             if world > 1:
                 dist.barrier()
@@ -646,7 +646,7 @@ def run_ours(args):
         conf = s.conf()
         e2e_iters = 10
         t_e2e = []
-        for rep in range(2):
+        for rep in range(3):
             torch.cuda.synchronize(dev)
             if world > 1:
                 dist.barrier()
