@@ -56,6 +56,7 @@ SIGNATURES = {
     "ddfan_HelicalToFan": (_i, [_p, _p, _p, _ll, _p, _i, _f, _f, _f, _i, _i, _f, _f, _i, _f, _f]),
     "ddfan_helical_to_fan_dev": (_i, [_p, _ll, _p, _i, _f, _f, _f, _i, _i, _f, _f, _i, _f, _f, _i, _p, _p,
                                       _p]),
+    "ddfan_ctpd_views_to_raw": (_i, [_p, _ll, _i, _i, _i, _p, _p]),
 }
 
 _LIB = None

@@ -222,6 +222,37 @@ __global__ void __launch_bounds__(256) k_rebin_routine(RebinParams p) {
   }
 }
 
+// DICOM-CT-PD stored pixels -> raw views: out[v'][k] = (float)pix[v][k],
+// v' = n - 1 - v when reversing (readProj.m:54 flips the view order), for the
+// W x H pixels k of a view (DICOM rows = detector columns, columns = detector
+// rows: already the [channel][row] layout).  8 pixels per thread and step.
+__global__ void __launch_bounds__(256) k_ctpd_views(const uint16_t* __restrict__ pix, long long n, long long per,
+                                                    int reverse, float* __restrict__ out) {
+  const long long total = n * per;
+  const long long stride = (long long)gridDim.x * blockDim.x * 8;
+  const bool vec = (per % 8) == 0;
+  for (long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 8; i < total; i += stride) {
+    const long long v = i / per, k = i - v * per;
+    const long long o = (reverse ? (n - 1 - v) : v) * per + k;
+    if (vec) {
+      const uint4 q = __ldg(reinterpret_cast<const uint4*>(pix + i));
+      const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+      float4 a, b;
+      a.x = (float)(w[0] & 0xffffu); a.y = (float)(w[0] >> 16);
+      a.z = (float)(w[1] & 0xffffu); a.w = (float)(w[1] >> 16);
+      b.x = (float)(w[2] & 0xffffu); b.y = (float)(w[2] >> 16);
+      b.z = (float)(w[3] & 0xffffu); b.w = (float)(w[3] >> 16);
+      reinterpret_cast<float4*>(out + o)[0] = a;
+      reinterpret_cast<float4*>(out + o)[1] = b;
+    } else {
+      for (int j = 0; j < 8 && i + j < total; ++j) {
+        const long long ij = i + j, vj = ij / per, kj = ij - vj * per;
+        out[(reverse ? (n - 1 - vj) : vj) * per + kj] = (float)pix[ij];
+      }
+    }
+  }
+}
+
 struct RebinHost {
   RebinParams p;
   std::vector<float> sm;
@@ -457,4 +488,20 @@ extern "C" DDFAN_API int ddfan_HelicalToFan(float* Proj, float* Views, const flo
   cudaStreamSynchronize(st);
   cudaStreamDestroy(st);
   return rc;
+}
+
+extern "C" DDFAN_API int ddfan_ctpd_views_to_raw(const uint16_t* d_pix, long long nViews, int W, int H, int reverse,
+                                                 float* d_proj, void* stream) {
+  if (!d_pix || !d_proj) return set_err(DDFAN_ERR_ARG, "ctpd_views_to_raw: null argument");
+  if (nViews < 1 || W < 1 || H < 1) return set_err(DDFAN_ERR_ARG, "ctpd_views_to_raw: bad sizes");
+  const long long per = (long long)W * H;
+  if ((per % 8) == 0 &&
+      ((reinterpret_cast<uintptr_t>(d_pix) & 15) != 0 || (reinterpret_cast<uintptr_t>(d_proj) & 15) != 0))
+    return set_err(DDFAN_ERR_ARG, "ctpd_views_to_raw: buffers must be 16-byte aligned");
+  const long long work = (nViews * per + 7) / 8;
+  const int blocks = (int)std::min<long long>((work + 255) / 256, 148LL * 8);
+  k_ctpd_views<<<std::max(blocks, 1), 256, 0, (cudaStream_t)stream>>>(d_pix, nViews, per, reverse ? 1 : 0, d_proj);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "ctpd_views_to_raw launch: %s", cudaGetErrorString(e));
+  return DDFAN_OK;
 }

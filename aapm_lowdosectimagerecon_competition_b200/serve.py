@@ -177,7 +177,7 @@ def pick_admission(queue_bytes, used, budget, backfill):
 
 
 class _Active:
-    __slots__ = ("req", "solver", "stream", "done", "out_dev", "out_host", "bytes", "t_admit")
+    __slots__ = ("req", "solver", "stream", "done", "out_dev", "out_host", "bytes", "t_admit", "iter_done")
 
 
 class Engine:
@@ -227,7 +227,14 @@ class Engine:
             # pinned host sinogram -> solver memory, asynchronous on the slot's stream
             a.solver.set_sinogram(inst.proj_host, stream=st)
             a.solver.set_image(torch.zeros((s.YN, s.XN, s.SLN), device=self.device), stream=st)
-            a.solver.iterate(inst.iters, use_graph=self.use_graph, stream=st)
+            # one graph replay per iteration, each followed by an event, so the
+            # progress of a solve in flight can be read without waiting for it
+            a.iter_done = []
+            for _ in range(inst.iters):
+                a.solver.iterate(1, use_graph=self.use_graph, stream=st)
+                ev = torch.cuda.Event()
+                ev.record(st)
+                a.iter_done.append(ev)
             a.out_dev = a.solver.image(stream=st)
             a.out_host = torch.empty(a.out_dev.shape, dtype=torch.float32, pin_memory=True)
             a.out_host.copy_(a.out_dev, non_blocking=True)
@@ -267,6 +274,15 @@ class Engine:
     def step(self):
         self._poll()
         self._admit()
+
+    def progress(self):
+        """(iterations, samples) completed so far by the solves still in flight."""
+        it = work = 0
+        for a in self.active:
+            n = sum(1 for ev in a.iter_done if ev.query())
+            it += n
+            work += n * a.req["inst"].work
+        return it, work
 
     def drain(self, poll_s=0.0005):
         while self.queue or self.active:
@@ -362,13 +378,20 @@ def run_serving(pool, engine, rate_hz=20.0, window_s=20.0, seed=5):
         if now >= window_s:
             break
         time.sleep(0.0005)
+    # iterations finished inside the window: whole solves plus the finished
+    # iterations of the solves still in flight
+    part_iters, part_work = engine.progress()
     done_in_window = [f for f in engine.finished if f["t_done"] - t0 <= window_s]
-    iters = sum(f["iters"] for f in done_in_window)
-    work = sum(f["iters"] * f["work"] for f in done_in_window)
+    iters = sum(f["iters"] for f in done_in_window) + part_iters
+    work = sum(f["iters"] * f["work"] for f in done_in_window) + part_work
     res = {"offered_rate_hz": arrivals.size / window_s, "served_rate_hz": len(done_in_window) / window_s,
            "arrived": int(arrivals.size), "served": len(done_in_window), "queued_at_end": len(engine.queue),
            "active_at_end": len(engine.active), "iters_per_s": iters / window_s,
-           "samples_per_s": work / window_s, "peak_active": engine.peak_active,
-           "peak_gb": engine.peak_used / 1e9, "window_s": window_s}
+           "samples_per_s": work / window_s, "in_flight_iters_counted": part_iters,
+           "peak_active": engine.peak_active, "peak_gb": engine.peak_used / 1e9, "window_s": window_s}
     res.update(latency_stats(done_in_window))
+    # requests still queued are dropped; the ones on the GPU finish before returning,
+    # so nothing of the window overlaps whatever runs next
+    engine.queue.clear()
+    engine.drain()
     return res

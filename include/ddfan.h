@@ -223,6 +223,17 @@ DDFAN_API int ddfan_helical_to_fan_dev(const float* d_proj, long long nViews, co
                                        float DetCenterW, float SpiralPitchFactor, int layout,
                                        float* d_Proj, float* d_Views, void* stream);
 
+/* DICOM-CT-PD projections on the device: the stored 16-bit pixels of nViews
+ * projection files, d_pix[nViews][W][H] (DICOM rows = detector columns W,
+ * DICOM columns = detector rows H), to the float raw views
+ * d_proj[nViews][W][H] that ddfan_helical_to_fan_dev reads, view order
+ * reversed when reverse != 0.  Replaces the conversion half of
+ * AAPM_script/readProj.m:43-54 (double(dicomread(...)), permute, flip); the
+ * files themselves are parsed on the host.  Buffers 16-byte aligned when
+ * W * H is a multiple of 8.  Stream-ordered. */
+DDFAN_API int ddfan_ctpd_views_to_raw(const uint16_t* d_pix, long long nViews, int W, int H, int reverse,
+                                      float* d_proj, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

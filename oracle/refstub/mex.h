@@ -1,7 +1,9 @@
 /* Minimal stand-in for MATLAB's mex.h, written for this repository.
- * It only lets the reference's MultiSlicesProjGPU.cu / MultiSlicesBackGPU.cu
- * translation units compile as plain CUDA objects; the MATLAB entry points
- * (mexFunction) are compiled but never called.  Test infrastructure only. */
+ * It only lets the reference's MultiSlicesProjGPU.cu / MultiSlicesBackGPU.cu /
+ * HelicalToFanFunc_mex.cpp translation units compile as plain objects (their
+ * mexFunction is compiled but never called) and the reference's cov_*.cpp
+ * byte converters run through oracle/ref_cov_harness.cpp.  Test
+ * infrastructure only. */
 #ifndef DDFAN_REFSTUB_MEX_H
 #define DDFAN_REFSTUB_MEX_H
 #include <stddef.h>
@@ -15,6 +17,7 @@ extern "C" {
 void* mxGetData(const mxArray*);
 double* mxGetPr(const mxArray*);
 mxArray* mxCreateNumericArray(mwSize, const mwSize*, mxClassID, mxComplexity);
+mxArray* mxCreateDoubleMatrix(mwSize, mwSize, mxComplexity);
 #ifdef __cplusplus
 }
 #endif
