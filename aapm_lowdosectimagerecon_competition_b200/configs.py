@@ -53,13 +53,16 @@ class Scan:
 
     def rebinned_hangs(self, spacing=36, BV=0.0):
         """Per-slice view angles (PN, SLN) as helical rebinning leaves them:
-        slice z starts at raw view 1 + spacing * z and its view ib has angle
-        mod((start + ib - 1) * delta + BV, 2 pi) in float32
+        slice z starts at raw view 1 + floor(spacing * z) and its view ib has
+        angle mod((start + ib - 1) * delta + BV, 2 pi) in float32
         (AAPM_script/HelicalToFanFunc_mex.cpp:77-81) -- one grid, circularly
-        shifted per slice, different in the last bits from slice to slice."""
+        shifted per slice, different in the last bits from slice to slice.
+        A non-integer spacing gives the irregular starts of slices at
+        linspace positions (reconscript.m:22)."""
         f = np.float32
         delta, twopi = f(2.0 * math.pi / self.PN), f(2.0 * math.pi)
-        i = (np.arange(self.PN)[:, None] + spacing * np.arange(self.SLN)[None, :]).astype(np.float32)
+        starts = np.floor(spacing * np.arange(self.SLN)).astype(np.int64)
+        i = (np.arange(self.PN)[:, None] + starts[None, :]).astype(np.float32)
         lam = (i * delta).astype(np.float32) + f(BV)
         # the reference's repeated float subtraction of 2 pi
         while True:

@@ -11,7 +11,42 @@
 #pragma once
 #include "ddfan_device.cuh"
 
+// Resident CTAs per SM the register allocation is sized for (256 threads each:
+// 4 -> at most 64 registers per thread, 2 -> 128).  Measured choices (96-view
+// c3 subset); overridable at build time for tuning sweeps.  The forward
+// projector with 48-byte cells (hi/lo, FP64) runs faster with 2 CTAs and 128
+// registers, which keep four lines of gathers in flight (3.69 -> 3.54 ms);
+// with 32-byte FP32 cells, or narrower z-tiles, 4 CTAs stay faster.
+#ifndef DDFAN_FWD_MIN_CTAS
+#define DDFAN_FWD_MIN_CTAS 4
+#endif
+#ifndef DDFAN_FWD_MIN_CTAS_WIDE
+#define DDFAN_FWD_MIN_CTAS_WIDE 2
+#endif
+#ifndef DDFAN_REF_MIN_CTAS
+#define DDFAN_REF_MIN_CTAS 3
+#endif
+#ifndef DDFAN_ADJ_MIN_CTAS
+#define DDFAN_ADJ_MIN_CTAS 4
+#endif
+// lines of a forward chunk unrolled together (more gathers in flight per thread)
+#ifndef DDFAN_FWD_LINE_UNROLL
+#define DDFAN_FWD_LINE_UNROLL 1
+#endif
+#ifndef DDFAN_FWD_LINE_UNROLL_WIDE
+#define DDFAN_FWD_LINE_UNROLL_WIDE 4
+#endif
+
 namespace ddfan {
+
+// per cell format M (SAT_FP32 = 32-byte cells; hi/lo and FP64 = 48-byte cells)
+// and z-tile width ZL: the wide setting only pays with 8 z-blocks per tile
+// (with 4, as per-slice-angle solves use, it cost 10 %)
+template <int M, int ZL> struct FwdTuning {
+  static constexpr bool wide = M != SAT_FP32 && ZL == 8;
+  static constexpr int min_ctas = wide ? DDFAN_FWD_MIN_CTAS_WIDE : DDFAN_FWD_MIN_CTAS;
+  static constexpr int line_unroll = wide ? DDFAN_FWD_LINE_UNROLL_WIDE : DDFAN_FWD_LINE_UNROLL;
+};
 
 // Stable partition of a call's views, x-major views first:
 // order[0, nx) are the x-major views, order[nx, PN) the others; counts = {nx, PN - nx}.
@@ -140,7 +175,7 @@ struct FwdTile {
 // FP64 boundary lines.  Phase A: a thread owns CG consecutive channels x 4
 // slices; channel u adds (Phi(c_{u+1}) - Phi(c_u)) / len_u on every line.
 template <int M, int ZL, int CG>
-__global__ void __launch_bounds__(256, 4) k_fwd(FwdArgs a) {
+__global__ void __launch_bounds__(256, FwdTuning<M, ZL>::min_ctas) k_fwd(FwdArgs a) {
   using T = FwdTile<ZL, CG>;
   constexpr int F4 = CellInfo<M>::F4;
   constexpr int NT = T::NT, CW = T::CW, NB = T::NB, CC = T::CC;
@@ -195,6 +230,7 @@ __global__ void __launch_bounds__(256, 4) k_fwd(FwdArgs a) {
       float part[CG][4];
 #pragma unroll
       for (int j = 0; j < CG; ++j) part[j][0] = part[j][1] = part[j][2] = part[j][3] = 0.f;
+#pragma unroll(FwdTuning<M, ZL>::line_unroll)
       for (int col = 0; col < ncol; ++col) {
         const float4* line = base + (size_t)(ii0 + col) * N * rowstride;
         Phi4<M> prev;
@@ -306,7 +342,7 @@ struct RefArgs {
 // (voxel, view) of the tile; phase A differences the two samples of the
 // channel prefix sums in table precision.  Lines are image rows (k = x).
 template <int M, int ZL>
-__global__ void __launch_bounds__(256, 3) k_back_ref(RefArgs a) {
+__global__ void __launch_bounds__(256, DDFAN_REF_MIN_CTAS) k_back_ref(RefArgs a) {
   using T = BackTile<ZL>;
   constexpr int F4 = CellInfo<M>::F4;
   constexpr int NT = T::NT, VG = T::VG, SPL = T::SPL, KT = T::KT, LT = T::LT, NV = T::NV;
@@ -417,7 +453,7 @@ struct AdjArgs {
 // consecutive pixels of a line (VG + 1 edges) x 4 slices.  XM selects the
 // lines (x columns for x-major views, y rows otherwise) and the views.
 template <int M, int ZL, bool XM>
-__global__ void __launch_bounds__(256, 4) k_back_adj(AdjArgs a) {
+__global__ void __launch_bounds__(256, DDFAN_ADJ_MIN_CTAS) k_back_adj(AdjArgs a) {
   using T = BackTile<ZL>;
   constexpr int F4 = CellInfo<M>::F4;
   constexpr int NT = T::NT, VG = T::VG, SPL = T::SPL, KT = T::KT, LT = T::LT, NE = T::NE;

@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--sat", default="hilo", choices=["fp32", "hilo", "fp64"])
     ap.add_argument("--back", default="adj", choices=["ref", "adj"])
     ap.add_argument("--slices", type=int, default=128)
+    ap.add_argument("--subsets", type=int, default=24, help="c3: ordered subsets (the configuration has 24)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
@@ -50,8 +51,9 @@ def parse():
     ap.add_argument("--config", default="c3", choices=["c3", "c4", "c5", "rebin"],
                     help="c3: the OS-SART contract line; c4: batched uneven reconstructions; "
                          "c5: Poisson-arrival serving")
-    ap.add_argument("--views", default="shared", choices=["shared", "rebinned"],
-                    help="c3: one angle list for all slices, or per-slice lists as rebinning makes them")
+    ap.add_argument("--views", default="shared", choices=["shared", "rebinned", "rebinned-irregular"],
+                    help="c3: one angle list for all slices, or per-slice lists as rebinning makes them "
+                         "(slices 36 raw views apart, or 86.07 apart as an AAPM-length scan gives)")
     ap.add_argument("--rotations", type=int, default=10, help="rebin: rotations of raw views")
     ap.add_argument("--rebin-slices", type=int, default=512, help="rebin: target slices")
     ap.add_argument("--instances", type=int, default=32)
@@ -366,7 +368,7 @@ def run_kernels(args):
     import torch
     from aapm_lowdosectimagerecon_competition_b200 import dd2, device
     dev = torch.device("cuda", 0)
-    s = workload(args.slices)
+    s = workload(args.slices, args.subsets)
     x0, y0, xds, yds = dd2.fan_geometry(s.sid, s.sdd, s.DNU, s.detCellWidth, s.detCntIdx)
     angs = torch.from_numpy(np.ascontiguousarray(s.angles()[::s.numOfOS])).to(dev)
     g = torch.Generator(device=dev)
@@ -396,9 +398,19 @@ def run_kernels(args):
                       "image": [s.XN, s.YN, s.SLN]}), flush=True)
 
 
-def workload(slices):
+def workload(slices, subsets=24):
     from aapm_lowdosectimagerecon_competition_b200 import configs
-    return configs.c3(SLN=slices)
+    s = configs.c3(SLN=slices)
+    s.numOfOS = subsets
+    return s
+
+
+def view_angles(s, views):
+    if views == "rebinned":
+        return s.rebinned_hangs(spacing=36)
+    if views == "rebinned-irregular":
+        return s.rebinned_hangs(spacing=86.07)
+    return s.hangs()
 
 
 def config_dict(s, args, n):
@@ -406,8 +418,10 @@ def config_dict(s, args, n):
                         (s.XN, s.YN, s.SLN, s.PN, s.DNU, s.numOfOS),
             "image": [s.XN, s.YN, s.SLN], "views": s.PN, "channels": s.DNU, "subsets": s.numOfOS,
             "sat": args.sat, "back": args.back, "instances": n,
-            "view_angles": "per-slice lists as helical rebinning makes them" if getattr(args, "views", "shared")
-                           == "rebinned" else "one list shared by all slices",
+            "view_angles": {"shared": "one list shared by all slices",
+                            "rebinned": "per-slice lists as helical rebinning makes them, slices 36 raw views apart",
+                            "rebinned-irregular": "per-slice lists as helical rebinning makes them, slices 86.07 "
+                                                  "raw views apart"}[getattr(args, "views", "shared")],
             "l2": "inputs larger than L2 (sinogram 868 MB, image 134 MB, prefix-sum tables 0.8 GB)",
             "parallelism": "one independent reconstruction per GPU (slices/requests shard with no exchange)"}
 
@@ -435,7 +449,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    s = workload(args.slices)
+    s = workload(args.slices, args.subsets)
     sample = 2
     from oracle import oracle as O
     O.build()
@@ -574,10 +588,10 @@ def run_ours(args):
                                 device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    s = workload(args.slices)
+    s = workload(args.slices, args.subsets)
     (x0, y0, xds, yds), xt, y = make_problem(s, dev, seed=7 + rank)
     mask = s.circular_mask()
-    hangs = s.rebinned_hangs() if args.views == "rebinned" else s.hangs()
+    hangs = view_angles(s, args.views)
     solver = device.OSSART(x0, y0, s.DNU, xds, yds, s.detCntIdx, hangs, s.XN, s.YN, s.SLN, s.dx,
                            mask=mask, numOfOS=s.numOfOS, useFISTA=s.useFISTA, nonneg=s.nonneg,
                            sat=args.sat, back=args.back, device=local)
@@ -630,6 +644,20 @@ def run_ours(args):
                 "kernel_ms_per_iter": {k: round(v[0], 3) for k, v in prof.items()},
                 "note": "achieved = algorithmic bytes per launch / CUDA-event launch time; the "
                         "path is gather/issue bound, not HBM bound"}
+    if top == "fwd" and args.views == "shared":
+        # the bound that applies: L1 gathers of prefix-sum cells -- per line of
+        # each ray group one cell per boundary (CG channels share CG + 1
+        # boundaries), a cell holding 4 slices (32 B FP32, 48 B hi/lo or FP64)
+        from aapm_lowdosectimagerecon_competition_b200 import _lib
+        cell = {"fp32": 32, "hilo": 48, "fp64": 48}[args.sat]
+        zl = int(_lib.load().ddfan_tune_get_zl((s.SLN + 3) // 4))
+        cg = 4 if zl >= 4 else (2 if zl == 2 else 1)
+        l1_bytes = (s.PN // s.numOfOS) * s.DNU * s.XN * ((s.SLN + 3) // 4) * (1.0 + 1.0 / cg) * cell
+        l1_peak = 148 * 128 * 1.965e9 / 1e12  # TB/s: 128 B per clock per SM at the maximum SM clock
+        l1_tbs = l1_bytes / (top_ms / 1e3) / 1e12
+        roofline["l1_gather"] = {"bytes_per_launch": l1_bytes, "achieved_tbs": l1_tbs, "peak_tbs": l1_peak,
+                                 "frac": l1_tbs / l1_peak,
+                                 "peak_source": "nominal L1 data bandwidth (148 SMs x 128 B/clk x 1.965 GHz)"}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
@@ -691,7 +719,7 @@ def _ossart_host(s, geom, y_h, x_h, out_h, mask, iters, args):
     import ctypes
     from aapm_lowdosectimagerecon_competition_b200._lib import BACK_MODES, SAT_MODES, call
     x0, y0, xds, yds = geom
-    hangs = np.ascontiguousarray(s.rebinned_hangs() if args.views == "rebinned" else s.hangs())
+    hangs = np.ascontiguousarray(view_angles(s, args.views))
     m = np.ascontiguousarray(mask, np.uint8)
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
     T = lambda t: ctypes.c_void_p(t.data_ptr())
