@@ -14,9 +14,9 @@
 // Resident CTAs per SM the register allocation is sized for (256 threads each:
 // 4 -> at most 64 registers per thread, 2 -> 128).  Measured choices (96-view
 // c3 subset); overridable at build time for tuning sweeps.  The forward
-// projector with 48-byte cells (hi/lo, FP64) runs faster with 2 CTAs and 128
-// registers, which keep four lines of gathers in flight (3.69 -> 3.54 ms);
-// with 32-byte FP32 cells, or narrower z-tiles, 4 CTAs stay faster.
+// projector with hi/lo cells runs faster with 2 CTAs and 128 registers, which
+// keep four lines of gathers in flight (3.69 -> 3.54 ms); with FP32 or FP64
+// cells, or narrower z-tiles, 4 CTAs stay faster.
 #ifndef DDFAN_FWD_MIN_CTAS
 #define DDFAN_FWD_MIN_CTAS 4
 #endif
@@ -39,11 +39,11 @@
 
 namespace ddfan {
 
-// per cell format M (SAT_FP32 = 32-byte cells; hi/lo and FP64 = 48-byte cells)
-// and z-tile width ZL: the wide setting only pays with 8 z-blocks per tile
-// (with 4, as per-slice-angle solves use, it cost 10 %)
+// per cell format M and z-tile width ZL: the wide setting only pays for hi/lo
+// cells on 8-block tiles (with 4 blocks, as per-slice-angle solves use, it
+// cost 10 %; with FP64 cells, whose double sums need more registers, 45 %)
 template <int M, int ZL> struct FwdTuning {
-  static constexpr bool wide = M != SAT_FP32 && ZL == 8;
+  static constexpr bool wide = M == SAT_HILO && ZL == 8;
   static constexpr int min_ctas = wide ? DDFAN_FWD_MIN_CTAS_WIDE : DDFAN_FWD_MIN_CTAS;
   static constexpr int line_unroll = wide ? DDFAN_FWD_LINE_UNROLL_WIDE : DDFAN_FWD_LINE_UNROLL;
 };
