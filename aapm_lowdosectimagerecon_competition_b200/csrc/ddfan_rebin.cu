@@ -40,6 +40,9 @@ struct RebinParams {
   const int* start;    // [SLN] floor((z - h/2) / deltaZ)
   float* out;
   float* views;
+  const int* sstart;   // [nsorted] starts >= 0 in ascending order
+  const int* sslice;   // [nsorted] their slices
+  int nsorted, chunks; // chunks: warps per raw view (32 slices each) to cover its slices
   int SLN, T, W, H;    // T = DefTimes
   float SD, SD2, PH, DCH, deltaZ, delta, BV, twopi, sm_lo, sm_hi;
 };
@@ -114,58 +117,66 @@ __device__ __forceinline__ float rebin_sample(const RebinParams& p, const RebinR
   return __fmul_rn(cosv, temp);
 }
 
-constexpr int kDiagViews = 32;  // raw views per CTA of k_rebin_diag
+// first index k in [0, n) with a[k] >= x (a ascending)
+__device__ __forceinline__ int lower_bound_int(const int* a, int n, long long x) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int m = (lo + hi) >> 1;
+    if ((long long)__ldg(a + m) < x) lo = m + 1;
+    else hi = m;
+  }
+  return lo;
+}
 
-// Mex layout out[s][ib][j], views[s][ib], traversed along raw views: a CTA
-// owns 32 consecutive slices (one per lane) and 32 consecutive raw views
-// (4 per warp).  For raw view i, lane s produces row ib = i - start_s of its
-// slice, so the 32 lanes read one detector column at 32 neighbouring heights
-// (a few sectors per load instead of one sector per lane) and the slice
-// blocks that need view i run side by side and share it in L2.  Each warp
-// gathers a 32-slice x 32-channel tile in shared memory and stores it as
-// 128-byte row pieces.  Rows this traversal never visits (raw view < 1) are
-// written by k_rebin_unvisited.
+// Mex layout out[s][ib][j], views[s][ib], traversed along raw views: warp
+// (view, chunk) takes raw view i and up to 32 of the slices that read it --
+// those with start in [i - T + 1, i], consecutive in start order -- one per
+// lane, each making its row ib = i - start.  The 32 lanes read one detector
+// column at neighbouring heights (a few sectors per load instead of one
+// sector per lane), every lane has work, and the warps of neighbouring raw
+// views run side by side and share those views in L2.  Each warp gathers a
+// 32-slice x 32-channel tile in shared memory and stores it as 128-byte row
+// pieces.  Rows no raw view >= 1 reaches are written by k_rebin_unvisited.
 template <bool VEC>
 __global__ void __launch_bounds__(256) k_rebin_diag(RebinParams p, long long vlo, long long vhi) {
   __shared__ float tile[8][32][33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int s = blockIdx.x * 32 + lane;
-  const bool sok = s < p.SLN;
-  const int st = sok ? p.start[s] : -1;
-  const float z = sok ? p.zpos[s] : 0.f;
+  const long long gw = (long long)blockIdx.x * 8 + warp;
+  const long long i = vlo + gw / p.chunks;  // 1-based raw view, >= vlo >= 1
+  const int q = (int)(gw % p.chunks);
+  if (i > vhi) return;  // uniform per warp; no block-wide barrier follows
+  const int a = lower_bound_int(p.sstart, p.nsorted, i - p.T + 1);
+  const int b = lower_bound_int(p.sstart, p.nsorted, i + 1);
+  const int k = a + 32 * q + lane;
+  const bool act = k < b;
+  const unsigned amask = __ballot_sync(0xffffffffu, act);
+  if (!amask) return;
+  const int s = act ? __ldg(p.sslice + k) : 0;
+  const int ib = act ? (int)(i - __ldg(p.sstart + k)) : 0;
   float(*t)[33] = tile[warp];
-  const long long i0 = vlo + (long long)blockIdx.y * kDiagViews;
-  for (int v = warp; v < kDiagViews; v += 8) {
-    const long long i = i0 + v;  // 1-based raw view, >= vlo >= 1
-    if (i > vhi) break;
-    const long long ibl = i - st;
-    const bool act = sok && st >= 0 && ibl >= 0 && ibl < p.T;
-    const unsigned amask = __ballot_sync(0xffffffffu, act);
-    if (!amask) continue;
-    const int ib = act ? (int)ibl : 0;
-    RebinRow r;
-    r.n = __fsub_rn(z, __fmul_rn((float)(i - 1), p.deltaZ));
-    float vtmp;
-    r.ok = act && rebin_in_rows(p, rebin_dv(p, r.n, p.sm_lo, &vtmp)) &&
-           rebin_in_rows(p, rebin_dv(p, r.n, p.sm_hi, &vtmp));
-    r.col = p.raw + (size_t)(i - p.view0) * p.W * p.H;
-    if (act) {
-      float lam = __fadd_rn(__fmul_rn((float)(i - 1), p.delta), p.BV);
-      while (lam > p.twopi) lam = __fsub_rn(lam, p.twopi);
-      p.views[(size_t)s * p.T + ib] = lam;
-    }
-    for (int j0 = 0; j0 < p.W; j0 += 32) {
-      const int nc = min(32, p.W - j0);
+  RebinRow r;
+  r.n = act ? __fsub_rn(__ldg(p.zpos + s), __fmul_rn((float)(i - 1), p.deltaZ)) : 0.f;
+  float vtmp;
+  r.ok = act && rebin_in_rows(p, rebin_dv(p, r.n, p.sm_lo, &vtmp)) &&
+         rebin_in_rows(p, rebin_dv(p, r.n, p.sm_hi, &vtmp));
+  r.col = p.raw + (size_t)(i - p.view0) * p.W * p.H;
+  if (act) {
+    float lam = __fadd_rn(__fmul_rn((float)(i - 1), p.delta), p.BV);
+    while (lam > p.twopi) lam = __fsub_rn(lam, p.twopi);
+    p.views[(size_t)s * p.T + ib] = lam;
+  }
+  for (int j0 = 0; j0 < p.W; j0 += 32) {
+    const int nc = min(32, p.W - j0);
 #pragma unroll 4
-      for (int c = 0; c < 32; ++c) t[lane][c] = (r.ok && c < nc) ? rebin_sample<VEC>(p, r, j0 + c) : 0.f;
-      __syncwarp();
-      for (unsigned m = amask; m; m &= m - 1) {
-        const int q = __ffs(m) - 1;
-        const int ibq = __shfl_sync(0xffffffffu, ib, q);
-        if (lane < nc) p.out[((size_t)(blockIdx.x * 32 + q) * p.T + ibq) * p.W + j0 + lane] = t[q][lane];
-      }
-      __syncwarp();
+    for (int c = 0; c < 32; ++c) t[lane][c] = (r.ok && c < nc) ? rebin_sample<VEC>(p, r, j0 + c) : 0.f;
+    __syncwarp();
+    for (unsigned m = amask; m; m &= m - 1) {
+      const int qq = __ffs(m) - 1;
+      const int sq = __shfl_sync(0xffffffffu, s, qq);
+      const int ibq = __shfl_sync(0xffffffffu, ib, qq);
+      if (lane < nc) p.out[((size_t)sq * p.T + ibq) * p.W + j0 + lane] = t[qq][lane];
     }
+    __syncwarp();
   }
 }
 
@@ -257,6 +268,7 @@ struct RebinHost {
   RebinParams p;
   std::vector<float> sm;
   std::vector<int> start;
+  std::vector<int> sstart, sslice;  // slices with start >= 0, by ascending start
   long long lo = 0, hi = -1;  // 1-based raw views the computed rows read (empty when hi < lo)
 };
 
@@ -312,8 +324,23 @@ int rebin_prepare(RebinHost& h, long long nViews, const float* zPos, int SLN, fl
     }
   }
   if (h.hi < h.lo) h.lo = 1, h.hi = 0;
+  // slices in start order, and how many of them one raw view serves at most
+  std::vector<int> idx;
+  for (int s = 0; s < SLN; ++s)
+    if (h.start[s] >= 0) idx.push_back(s);
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return h.start[a] < h.start[b]; });
+  h.sslice = idx;
+  h.sstart.resize(idx.size());
+  for (size_t k = 0; k < idx.size(); ++k) h.sstart[k] = h.start[idx[k]];
+  int most = 0;
+  for (size_t k0 = 0, k1 = 0; k0 < idx.size(); ++k0) {
+    while (k1 < idx.size() && (long long)h.sstart[k1] <= (long long)h.sstart[k0] + DefTimes - 1) ++k1;
+    most = std::max(most, (int)(k1 - k0));
+  }
   RebinParams& p = h.p;
   p = RebinParams{};
+  p.nsorted = (int)idx.size();
+  p.chunks = std::max(1, (most + 31) / 32);
   p.SLN = SLN; p.T = DefTimes; p.W = DetWidth; p.H = DetHeight;
   p.SD = SD; p.SD2 = SD * SD; p.PH = PerDetH; p.DCH = DetCenterHreal;
   p.deltaZ = deltaZ; p.delta = delta; p.BV = BVAngle; p.twopi = (float)(2 * M_PI);
@@ -329,13 +356,13 @@ int rebin_launch(const RebinHost& h, int layout, cudaStream_t st) {
   const bool vec = p.H % 4 == 0 && (reinterpret_cast<uintptr_t>(p.raw) & 15) == 0;
   if (layout == 0) {
     k_rebin_unvisited<<<p.SLN, 256, 0, st>>>(p);
-    if (h.hi >= h.lo) {
-      const long long nchunk = (h.hi - h.lo + kDiagViews) / kDiagViews;
-      if (nchunk > 65535)
+    if (h.hi >= h.lo && p.nsorted > 0) {
+      const long long warps = (h.hi - h.lo + 1) * (long long)p.chunks;
+      const long long ctas = (warps + 7) / 8;
+      if (ctas > 0x7fffffffLL)
         return set_err(DDFAN_ERR_UNSUPPORTED, "HelicalToFan: %lld raw views in one call", h.hi - h.lo + 1);
-      dim3 grid((p.SLN + 31) / 32, (unsigned)nchunk);
-      if (vec) k_rebin_diag<true><<<grid, 256, 0, st>>>(p, h.lo, h.hi);
-      else k_rebin_diag<false><<<grid, 256, 0, st>>>(p, h.lo, h.hi);
+      if (vec) k_rebin_diag<true><<<(unsigned)ctas, 256, 0, st>>>(p, h.lo, h.hi);
+      else k_rebin_diag<false><<<(unsigned)ctas, 256, 0, st>>>(p, h.lo, h.hi);
     }
   } else {
     dim3 grid(p.T, (p.SLN + 31) / 32);
@@ -365,7 +392,8 @@ int rebin_tables(RebinHost& h, const float* zPos, void** buf, cudaStream_t st) {
   const int W = h.p.W, SLN = h.p.SLN;
   const size_t b_sm = ((sizeof(float) * W + 255) / 256) * 256;
   const size_t b_z = ((sizeof(float) * SLN + 255) / 256) * 256;
-  const size_t bytes = b_sm + b_z + sizeof(int) * SLN;
+  const size_t b_i = ((sizeof(int) * SLN + 255) / 256) * 256;
+  const size_t bytes = b_sm + b_z + 3 * b_i;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxStagingDevices) {
     cudaGetLastError();
@@ -390,6 +418,10 @@ int rebin_tables(RebinHost& h, const float* zPos, void** buf, cudaStream_t st) {
     std::memcpy(sg.host, h.sm.data(), sizeof(float) * W);
     std::memcpy(sg.host + b_sm, zPos, sizeof(float) * SLN);
     std::memcpy(sg.host + b_sm + b_z, h.start.data(), sizeof(int) * SLN);
+    if (!h.sstart.empty()) {
+      std::memcpy(sg.host + b_sm + b_z + b_i, h.sstart.data(), sizeof(int) * h.sstart.size());
+      std::memcpy(sg.host + b_sm + b_z + 2 * b_i, h.sslice.data(), sizeof(int) * h.sslice.size());
+    }
     e = cudaMemcpyAsync(b, sg.host, bytes, cudaMemcpyHostToDevice, st);
   }
   if (e == cudaSuccess) e = cudaEventRecord(sg.copied, st);
@@ -402,6 +434,8 @@ int rebin_tables(RebinHost& h, const float* zPos, void** buf, cudaStream_t st) {
   h.p.sm = reinterpret_cast<const float*>(b);
   h.p.zpos = reinterpret_cast<const float*>(b + b_sm);
   h.p.start = reinterpret_cast<const int*>(b + b_sm + b_z);
+  h.p.sstart = reinterpret_cast<const int*>(b + b_sm + b_z + b_i);
+  h.p.sslice = reinterpret_cast<const int*>(b + b_sm + b_z + 2 * b_i);
   return DDFAN_OK;
 }
 
