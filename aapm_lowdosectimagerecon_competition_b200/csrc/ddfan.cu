@@ -401,8 +401,13 @@ template <int M, int ZL>
 static void fwd_go(const FwdArgs& a, int nzt, cudaStream_t st) {
   constexpr int CG = FwdCG<ZL>::v;
   using T = FwdTile<ZL, CG>;
-  dim3 grid((a.U + T::CW - 1) / T::CW, a.PN, nzt);
-  k_fwd<M, ZL, CG><<<grid, T::NT, 0, st>>>(a);
+  constexpr int kMaxRows = 65535;  // grid y limit
+  for (int r0 = 0; r0 < a.PN; r0 += kMaxRows) {
+    FwdArgs b = a;
+    b.row0 = r0;
+    dim3 grid((a.U + T::CW - 1) / T::CW, std::min(a.PN - r0, kMaxRows), nzt);
+    k_fwd<M, ZL, CG><<<grid, T::NT, 0, st>>>(b);
+  }
 }
 
 template <int M>
@@ -418,8 +423,8 @@ static void fwd_zl(int ZL, const FwdArgs& a, int nzt, cudaStream_t st) {
 int launch_fwd(const Plan& p, const ViewGeom* vg, const double2* fc, const float* cvd,
                const int* order, int PN, float* d_prj, int zlo, int zhi, cudaStream_t st,
                const int4* ztd) {
-  if (PN > 65535) return set_err(DDFAN_ERR_UNSUPPORTED, "more than 65535 views in one call");
   FwdArgs a;
+  a.row0 = 0;
   a.ztd = ztd;
   a.satx = p.d_satx; a.saty = p.d_saty; a.vg = vg; a.fc = fc; a.cvd = cvd; a.order = order;
   a.out = d_prj; a.PN = PN; a.U = p.U; a.Z = p.Z; a.ZB = p.ZB; a.XN = p.XN; a.YN = p.YN;

@@ -62,10 +62,11 @@ extern "C" DDFAN_API int ddfan_proj_noalloc(float x0, float y0, int DNU, const f
                                             const float* d_vol, float dx, const uint8_t* mask,
                                             int sat_mode, float* d_prj, void* stream) {
   if (!xds || !yds || !d_angs || !d_vol || !d_prj) return set_err(DDFAN_ERR_ARG, "proj_noalloc: null argument");
-  if (DNU < 2 || DNU + 1 > 1024 || XN < 1 || YN < 1 || XN > 1024 || YN > 1024 || SLN < 1 || PN < 1 ||
-      PN > 65535)
+  if (DNU < 2 || XN < 1 || YN < 1 || SLN < 1 || PN < 1)
     return set_err(DDFAN_ERR_ARG, "proj_noalloc: bad sizes (DNU=%d XN=%d YN=%d SLN=%d PN=%d)", DNU, XN, YN,
                    SLN, PN);
+  if (XN > 1024 || YN > 1024 || DNU + 1 > 1024)
+    return set_err(DDFAN_ERR_UNSUPPORTED, "proj_noalloc: lines longer than 1024 cells are not supported");
   if (!(dx > 0.f)) return set_err(DDFAN_ERR_ARG, "proj_noalloc: dx must be > 0");
   if (sat_mode < SAT_FP32 || sat_mode > SAT_FP64) return set_err(DDFAN_ERR_ARG, "proj_noalloc: sat_mode %d", sat_mode);
   int dev = 0;

@@ -157,6 +157,7 @@ struct FwdArgs {
   int zlo, zhi;        // slices written
   int zt0;             // z-tile of grid z-index 0 (the grid covers the tiles of [zlo, zhi))
   const int4* ztd;     // per z-tile view ranges, or null
+  int row0;            // CTA row of grid y-index 0 (views beyond 65535 go in further launches)
 };
 
 template <int ZL, int CG>
@@ -186,8 +187,9 @@ __global__ void __launch_bounds__(256, FwdTuning<M, ZL>::min_ctas) k_fwd(FwdArgs
   const int zl = tid % ZL, g = tid / ZL;
   const int zt = blockIdx.z + a.zt0;
   const ZtRange rg = zt_range(a.ztd, zt, a.PN, nullptr);
-  if ((int)blockIdx.y >= rg.count) return;  // uniform per CTA
-  const int slot = a.order ? a.order[rg.ooff + blockIdx.y] : blockIdx.y;
+  const int row = a.row0 + (int)blockIdx.y;
+  if (row >= rg.count) return;  // uniform per CTA
+  const int slot = a.order ? a.order[rg.ooff + row] : row;
   const int p = rg.gbase + slot;  // geometry row
   const int zb = zt * ZL + zl;
   const int ub0 = blockIdx.x * CW;

@@ -521,7 +521,6 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
         W = t;
       }
     }
-    if (W.PNmax > 65535) return set_err(DDFAN_ERR_UNSUPPORTED, "solver: %d views in one z-tile range", W.PNmax);
     s.Zi = W.Zi; s.nzt = W.nzt; s.Mc = W.Mc; s.perm = W.perm; s.maxcnt = W.maxcnt;
   } else {
     s.Zi = SLN;

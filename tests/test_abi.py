@@ -75,6 +75,33 @@ def test_no_gpu_fails_loudly():
     assert "CUDA" in str(e.value) or "device" in str(e.value)
 
 
+@pytest.mark.parametrize("XN,YN,DNU,code", [(1025, 64, 64, 4), (64, 1025, 64, 4), (64, 64, 1024, 4),
+                                            (1024, 1024, 1023, None)])
+def test_line_length_limit_is_checked_before_device_work(XN, YN, DNU, code):
+    """Image lines and detector rows of up to 1024 cells; longer ones return
+    DDFAN_ERR_UNSUPPORTED from plan creation and the no-alloc projection,
+    before any device is touched (so the same on a machine without one)."""
+    lib = _lib.load()
+    x0, y0, xds, yds = dd2.fan_geometry(np.float32(595.0), np.float32(1085.6), DNU, np.float32(1.2858),
+                                        np.float32((DNU + 1) / 2.0))
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    h = ctypes.c_void_p()
+    rc = lib.ddfan_plan_create(ctypes.byref(h), x0, y0, DNU, P(xds), P(yds), (DNU + 1) / 2.0, 0.0, 0.0, XN, YN,
+                               0.7, None, 8, 96, 1, 0)
+    if h.value:
+        lib.ddfan_plan_destroy(h)
+    dummy = np.zeros(4, np.float32)
+    rc2 = lib.ddfan_proj_noalloc(x0, y0, DNU, P(xds), P(yds), 0.0, 0.0, P(dummy), 96, XN, YN, 8, P(dummy), 0.7,
+                                 None, 1, P(dummy), None)
+    if code is None:  # at the limit: passes the size check (then needs a device)
+        assert rc != 4 and rc2 != 4
+        if not torch.cuda.is_available():
+            assert rc == 2 and rc2 == 2
+    else:
+        assert rc == code and rc2 == code
+        assert b"1024" in lib.ddfan_last_error()
+
+
 def test_argument_validation_before_any_device_work():
     s = configs.scaled(configs.c2(SLN=2), XN=16, DNU=24, PN=8)
     x0, y0, xds, yds = dd2.fan_geometry(s.sid, s.sdd, s.DNU, s.detCellWidth, s.detCntIdx)
