@@ -37,6 +37,8 @@ SIGNATURES = {
     "ddfan_plan_create": (_i, [_p, _f, _f, _i, _p, _p, _f, _f, _f, _i, _i, _f, _p, _i, _i, _i, _i]),
     "ddfan_plan_destroy": (None, [_p]),
     "ddfan_plan_device_bytes": (_sz, [_p]),
+    "ddfan_cached_bytes": (_sz, [_i]),
+    "ddfan_release_cached": (_i, [_i]),
     "ddfan_proj_dev": (_i, [_p, _p, _i, _i, _p, _p, _p]),
     "ddfan_back_dev": (_i, [_p, _p, _i, _i, _p, _p, _i, _p]),
     "ddfan_proj_noalloc": (_i, [_f, _f, _i, _p, _p, _f, _f, _p, _i, _i, _i, _i, _p, _f, _p, _i, _p, _p]),

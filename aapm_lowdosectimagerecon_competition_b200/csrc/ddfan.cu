@@ -98,16 +98,56 @@ int pow2_zl(int ZB) {
   return best;
 }
 
-// Stream-ordered device memory (cudaMallocAsync / cudaFreeAsync from the
-// device's default pool): creating or destroying a plan or a solver never
-// synchronises the device, so other solves keep running meanwhile.
+// Stream-ordered device memory from one pool per device owned by the
+// library: creating or destroying a plan or a solver never synchronises the
+// device, so other solves keep running meanwhile.  The pool keeps the blocks
+// that destroyed plans and solvers free (release threshold: unlimited) and
+// serves the next ones from them; the device's default pool returns freed
+// memory to the driver at every synchronisation, and mapping it again cost
+// 30 ms to 1 s per gigabyte-sized solve.  ddfan_release_cached hands the
+// unused part back.
+static std::mutex g_pool_mutex;
+static std::map<int, cudaMemPool_t> g_pools;
+
+static cudaMemPool_t lib_pool(int dev, bool create) {
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  auto it = g_pools.find(dev);
+  if (it != g_pools.end()) return it->second;
+  if (!create) return nullptr;
+  cudaMemPoolProps props;
+  std::memset(&props, 0, sizeof(props));
+  props.allocType = cudaMemAllocationTypePinned;
+  props.handleTypes = cudaMemHandleTypeNone;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t pool = nullptr;
+  if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  uint64_t keep = ~0ull;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  g_pools[dev] = pool;
+  return pool;
+}
+
 int dev_alloc(void** p, size_t bytes, cudaStream_t st) {
   *p = nullptr;
-  cudaError_t e = cudaMallocAsync(p, std::max<size_t>(bytes, 1), st);
+  bytes = std::max<size_t>(bytes, 1);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaMemPool_t pool = lib_pool(dev, true);
+  cudaError_t e = pool ? cudaMallocFromPoolAsync(p, bytes, pool, st) : cudaMallocAsync(p, bytes, st);
+  if (e == cudaErrorMemoryAllocation && pool) {
+    // cached blocks too fragmented for this request: give them back, retry once
+    cudaGetLastError();
+    cudaMemPoolTrimTo(pool, 0);
+    e = cudaMallocFromPoolAsync(p, bytes, pool, st);
+  }
   if (e != cudaSuccess) {
     *p = nullptr;
     cudaGetLastError();
-    return set_err(DDFAN_ERR_NOMEM, "cudaMallocAsync(%zu bytes): %s", bytes, cudaGetErrorString(e));
+    return set_err(DDFAN_ERR_NOMEM, "cudaMallocFromPoolAsync(%zu bytes): %s", bytes, cudaGetErrorString(e));
   }
   return DDFAN_OK;
 }
@@ -686,6 +726,38 @@ DDFAN_API int ddfan_plan_create(ddfan_plan** out, float x0, float y0, int DNU, c
 }
 
 DDFAN_API void ddfan_plan_destroy(ddfan_plan* plan) { plan_free(reinterpret_cast<Plan*>(plan)); }
+
+DDFAN_API size_t ddfan_cached_bytes(int device) {
+  cudaMemPool_t pool = lib_pool(device, false);
+  if (!pool) return 0;
+  uint64_t reserved = 0, used = 0;
+  if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess ||
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return reserved > used ? (size_t)(reserved - used) : 0;
+}
+
+DDFAN_API int ddfan_release_cached(int device) {
+  cudaMemPool_t pool = lib_pool(device, false);
+  if (!pool) return DDFAN_OK;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(DDFAN_ERR_ARG, "release_cached: device %d", device);
+  }
+  // blocks whose stream-ordered free has not completed yet are not unused
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemPoolTrimTo(pool, 0);
+  if (prev >= 0) cudaSetDevice(prev);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(DDFAN_ERR_CUDA, "release_cached: %s", cudaGetErrorString(e));
+  }
+  return DDFAN_OK;
+}
 
 DDFAN_API size_t ddfan_plan_device_bytes(const ddfan_plan* plan) {
   return plan ? reinterpret_cast<const Plan*>(plan)->bytes : 0;

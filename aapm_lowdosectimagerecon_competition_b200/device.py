@@ -26,6 +26,20 @@ def _stream(stream):
     return ctypes.c_void_p(stream.cuda_stream)
 
 
+def cached_bytes(device=None):
+    """Device bytes the library's memory pool holds unused (freed by
+    destroyed plans and solvers, kept for the next ones)."""
+    d = torch.cuda.current_device() if device is None else int(device)
+    return int(load().ddfan_cached_bytes(d))
+
+
+def release_cached(device=None):
+    """Return the pool's unused device memory to the driver (synchronises
+    the device)."""
+    d = torch.cuda.current_device() if device is None else int(device)
+    call("ddfan_release_cached", d)
+
+
 class Plan:
     """Geometry + scratch for repeated projections of one shape
     (ddfan_plan_create; replaces the per-call set-up of the reference's

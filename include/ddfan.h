@@ -116,6 +116,15 @@ DDFAN_API void ddfan_plan_destroy(ddfan_plan* plan);
 /* device bytes held by the plan */
 DDFAN_API size_t ddfan_plan_device_bytes(const ddfan_plan* plan);
 
+/* Plans, solvers and rebinning calls take device memory, stream-ordered,
+ * from one pool per device that the library owns; memory they free stays
+ * in that pool for the next ones (no new mapping per solve).  Bytes the
+ * pool holds unused, and a call that returns them to the driver (it
+ * synchronises the device first).  No reference counterpart: the mex
+ * functions allocate and free on every call. */
+DDFAN_API size_t ddfan_cached_bytes(int device);
+DDFAN_API int ddfan_release_cached(int device);
+
 /* Forward projection of device vol[YN][XN][SLN] into device prj[PN][DNU][SLN].
  * d_angs: device view angles; angs_per_slice = 0: d_angs[PN] shared by all
  * slices; 1: d_angs[PN][SLN] (the reference's hangs layout; slices whose
