@@ -422,44 +422,27 @@ static void win_layout(const std::vector<int>& off, int NG, int T, int nOS, int 
   }
 }
 
-// Row sums and column sums of every subset from slice 0's angles
-// (AAPM_script/OSSART_AAPM.m:57-66).  A one-slice launch fills a small part of
-// the GPU (a 512 x 512 backprojection is 128 CTAs), so the subsets run side by
-// side: the row sums of all views in one forward launch, the column sums on up
-// to kWeightStreams streams, each with its own one-slice plan (the plans'
-// sinogram tables are per-launch scratch).
-static constexpr int kWeightStreams = 8;
-
-struct SideStream {
-  cudaStream_t s = nullptr;
-  cudaEvent_t done = nullptr;
-  ~SideStream() {
-    if (done) cudaEventDestroy(done);
-    if (s) cudaStreamDestroy(s);
-  }
-};
-
+// Row sums and column sums of every subset from slice 0's angles, on a
+// one-slice plan (AAPM_script/OSSART_AAPM.m:57-66).  The row sums of all views
+// go in one forward launch (views are independent; one subset's launch fills
+// a small part of the GPU).  The column sums stay one subset at a time on the
+// solver's stream: spreading them over side streams cut a lone solver's
+// set-up by 5 ms but cost batched solves 20 % of their throughput, as those
+// latency-bound one-slice launches took SM slots from the other solves.
 static int solver_weights(Solver& s, const PlanDesc& d, const std::vector<float>& angs0, int PNmax, cudaStream_t st) {
   const int XN = s.XN, YN = s.YN, DNU = s.U, P = s.PNall;
-  const int NW = std::min(s.nsub, kWeightStreams);
   PlanDesc d1 = d;
   d1.SLN = 1;
   d1.PNmax = PNmax;
   d1.zl_force = 0;
-  std::vector<PlanPtr> P1(NW);
-  std::vector<SideStream> ws(NW);
-  for (int i = 0; i < NW; ++i) {
-    int rc = plan_create(&P1[i].p, d1);
-    if (rc) return rc;
-    DDFAN_CK(cudaStreamCreateWithFlags(&ws[i].s, cudaStreamNonBlocking));
-    DDFAN_CK(cudaEventCreateWithFlags(&ws[i].done, cudaEventDisableTiming));
-  }
+  PlanPtr P1;
+  int rc = plan_create(&P1.p, d1);
+  if (rc) return rc;
   DevBuf<ViewGeom> vg(st);
   DevBuf<double2> fc(st);
   DevBuf<float> cvd(st), ang(st), ones(st);
   DevBuf<int> order(st), counts(st), order_all(st), counts_all(st);
   const size_t n1 = std::max((size_t)XN * YN, (size_t)PNmax * DNU);
-  int rc;
   if ((rc = vg.alloc(P)) || (rc = fc.alloc((size_t)P * (DNU + 1))) || (rc = cvd.alloc((size_t)P * DNU)) ||
       (rc = ang.alloc(P)) || (rc = ones.alloc(n1)) || (rc = order.alloc(P)) || (rc = counts.alloc(2 * (size_t)s.nsub)) ||
       (rc = order_all.alloc(P)) || (rc = counts_all.alloc(2)))
@@ -467,50 +450,27 @@ static int solver_weights(Solver& s, const PlanDesc& d, const std::vector<float>
   std::vector<float> h1(n1, 1.0f);
   DDFAN_CK(cudaMemcpyAsync(ones.p, h1.data(), sizeof(float) * n1, cudaMemcpyHostToDevice, st));
   DDFAN_CK(cudaMemcpyAsync(ang.p, angs0.data(), sizeof(float) * P, cudaMemcpyHostToDevice, st));
-  if ((rc = launch_view_geom(*P1[0].p, ang.p, 1, P, vg.p, fc.p, cvd.p, st))) return rc;
+  if ((rc = launch_view_geom(*P1.p, ang.p, 1, P, vg.p, fc.p, cvd.p, st))) return rc;
   for (int k = 0; k < s.nsub; ++k)
     if ((rc = launch_view_order(vg.p + s.off[k], s.cnt[k], order.p + s.off[k], counts.p + 2 * k, st))) return rc;
   if ((rc = launch_view_order(vg.p, P, order_all.p, counts_all.p, st))) return rc;
-  cudaEvent_t fork = nullptr;
-  DDFAN_CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
-  cudaEventRecord(fork, st);
+  if ((rc = launch_sat_image(*P1.p, ones.p, st))) return rc;
+  if ((rc = launch_fwd(*P1.p, vg.p, fc.p, cvd.p, order_all.p, P, s.d_rows, 0, 1, st))) return rc;
   const bool adj = s.back_mode == DDFAN_BACK_ADJ;
-  auto side_work = [&]() -> int {
-    int r;
-    for (int i = 0; i < NW; ++i) {
-      DDFAN_CK(cudaStreamWaitEvent(ws[i].s, fork, 0));
-      if ((r = launch_sat_image(*P1[i].p, ones.p, ws[i].s))) return r;
-    }
-    // row sums of every view: views are independent, one launch
-    if ((r = launch_fwd(*P1[0].p, vg.p, fc.p, cvd.p, order_all.p, P, s.d_rows, 0, 1, ws[0].s))) return r;
-    for (int k = 0; k < s.nsub; ++k) {
-      const int i = (k + 1) % NW;  // the row-sum launch occupies stream 0 first
-      const Plan& q = *P1[i].p;
-      const int o = s.off[k], c = s.cnt[k];
-      if ((r = launch_sat_sino(q, ones.p, c, adj ? cvd.p + (size_t)o * DNU : nullptr, 1.f, nullptr, nullptr,
-                               nullptr, ws[i].s)))
-        return r;
-      BackEpi e{};
-      e.out = s.d_cols + (size_t)k * XN * YN;
-      e.mask = q.has_mask ? q.d_mask : nullptr;
-      e.zlo = 0; e.zhi = 1;
-      if ((r = launch_back(q, s.back_mode, vg.p + o, fc.p + (size_t)o * (DNU + 1), order.p + o, counts.p + 2 * k,
-                           c, e, ws[i].s)))
-        return r;
-    }
-    return DDFAN_OK;
-  };
-  rc = side_work();
-  // join every side stream (also after an error: the buffers above are
-  // released on st and must outlive the work already queued)
-  for (int i = 0; i < NW; ++i) {
-    cudaEventRecord(ws[i].done, ws[i].s);
-    cudaStreamWaitEvent(st, ws[i].done, 0);
+  for (int k = 0; k < s.nsub; ++k) {
+    const int o = s.off[k], c = s.cnt[k];
+    if ((rc = launch_sat_sino(*P1.p, ones.p, c, adj ? cvd.p + (size_t)o * DNU : nullptr, 1.f, nullptr, nullptr,
+                              nullptr, st)))
+      return rc;
+    BackEpi e{};
+    e.out = s.d_cols + (size_t)k * XN * YN;
+    e.mask = P1.p->has_mask ? P1.p->d_mask : nullptr;
+    e.zlo = 0; e.zhi = 1;
+    if ((rc = launch_back(*P1.p, s.back_mode, vg.p + o, fc.p + (size_t)o * (DNU + 1), order.p + o,
+                          counts.p + 2 * k, c, e, st)))
+      return rc;
   }
-  cudaEventDestroy(fork);
-  const cudaError_t e = cudaStreamSynchronize(st);
-  if (rc) return rc;
-  if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "solver weights: %s", cudaGetErrorString(e));
+  DDFAN_CK(cudaStreamSynchronize(st));
   return DDFAN_OK;
 }
 
@@ -691,9 +651,8 @@ DDFAN_API size_t ddfan_ossart_estimate_bytes(int XN, int YN, int DNU, int SLN, i
                      3 * P * sizeof(int) + 2 * (size_t)numOfOS * sizeof(int) + P * U * sizeof(float) +
                      (size_t)numOfOS * XN * YN * sizeof(float) + P * U * SLN * sizeof(float) +
                      2 * V * sizeof(float) + PNmax * U * SLN * sizeof(float) + sizeof(double);
-  // transient at creation: the one-slice weight plans and their buffers
-  const size_t NW = (size_t)std::min(numOfOS, kWeightStreams);
-  const size_t weights = NW * ddfan_plan_estimate_bytes(XN, YN, DNU, 1, (int)PNmax, sat_mode) +
+  // transient at creation: the one-slice weight plan and its buffers
+  const size_t weights = ddfan_plan_estimate_bytes(XN, YN, DNU, 1, (int)PNmax, sat_mode) +
                          P * sizeof(ViewGeom) + P * (U + 1) * sizeof(double2) +
                          (std::max((size_t)XN * YN, PNmax * U) + P * U + 3 * P + 2 * (size_t)numOfOS + 2) * sizeof(float);
   return plan + own + weights;
