@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <unordered_map>
@@ -13,6 +14,7 @@
 #include "ddfan.h"
 #include "ddfan_kernels.cuh"
 #include "ddfan_plan.h"
+#include "ddfan_ps_kernels.cuh"
 
 namespace ddfan {
 
@@ -194,8 +196,20 @@ struct Solver {
   int* d_soff = nullptr;     // internal slice -> window offset (INT_MAX for padding)
   int4* d_ztd = nullptr;     // [nsub][nzt] view ranges
   std::vector<int> maxcnt;   // per subset: largest range of a z-tile
-  float* d_xu = nullptr;     // [YN][XN][Z] image in the caller's slice order
-  float* d_stage = nullptr;  // [PNall][U][Z] host sinogram staging (windowed)
+  float* d_xu = nullptr;     // [YN][XN][Z] image in the caller's layout
+  float* d_stage = nullptr;  // [PNall][U][Z] host sinogram staging (windowed, slice-major)
+  // Per-slice view angles, slice-major path: every slice keeps its own
+  // geometry (rows z * cstride + m: view k + m * numOfOS of slice z in
+  // subset k, rebuilt per subset) and the image, sinogram and prefix-sum
+  // tables are slice-major: d_x [Z][YN][XN], d_y [Z][PNall][U],
+  // d_ax [Z][cstride][U].
+  bool ps = false;
+  int cstride = 0;
+  float* d_pang = nullptr;   // [nsub][Z][cstride] angles of each slice's views per subset
+  float* d_xt = nullptr;     // [Z][XN][YN] image columns
+  float* d_tabx = nullptr;   // image rows table [Z][YN][XN] cells
+  float* d_taby = nullptr;   // image columns table [Z][XN][YN] cells
+  float* d_sq = nullptr;     // weighted residual table [Z][cstride][U+1] cells
   cudaStream_t own = nullptr;
   cudaEvent_t last_use = nullptr;  // recorded after work enqueued on a caller's stream
   cudaGraph_t graph = nullptr;
@@ -219,7 +233,7 @@ static void solver_free(Solver* s) {
   if (s->graph) cudaGraphDestroy(s->graph);
   void* ptrs[] = {s->d_vg, s->d_fc, s->d_cvd, s->d_yview, s->d_order, s->d_counts, s->d_rows, s->d_cols,
                   s->d_y, s->d_x, s->d_xprev, s->d_ax, s->d_t, s->d_perm, s->d_inv, s->d_soff, s->d_ztd,
-                  s->d_xu, s->d_stage};
+                  s->d_xu, s->d_stage, s->d_pang, s->d_xt, s->d_tabx, s->d_taby, s->d_sq};
   for (void* q : ptrs) dev_free(q, s->own);
   if (s->own) cudaStreamDestroy(s->own);
   if (s->last_use) cudaEventDestroy(s->last_use);
@@ -259,12 +273,139 @@ static int gather_slices(const float* src, int Zs, float* dst, int Zd, const int
   return DDFAN_OK;
 }
 
+// ------------------------------------------------------------ slice-major path
+
+static int ps_check(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "%s launch: %s", what, cudaGetErrorString(e));
+  return DDFAN_OK;
+}
+
+// out[b][c][r] = in[b][r][c]
+static int ps_transpose(const float* in, float* out, int B, long long R, int C, cudaStream_t st) {
+  if (B < 1 || R < 1 || C < 1) return DDFAN_OK;
+  const long long nrt = (R + 31) / 32;
+  dim3 grid((C + 31) / 32, (unsigned)std::min<long long>(nrt, 65535), B);
+  k_ps_transpose<<<grid, 256, 0, st>>>(in, out, R, C);
+  return ps_check("k_ps_transpose");
+}
+
+template <int M, int C, int KIND>
+static void ps_scan_c(const PsScanArgs& a, cudaStream_t st) {
+  constexpr int WPC = C > 24 ? 2 : 4;  // warps (lines) per CTA, as k_ps_scan
+  k_ps_scan<M, C, KIND><<<(a.nlines + WPC - 1) / WPC, 32 * WPC, 0, st>>>(a);
+}
+
+template <int M, int KIND>
+static void ps_scan_go(const PsScanArgs& a, cudaStream_t st) {
+  const int C = (a.Nw + 31) / 32;
+  if (C <= 8) ps_scan_c<M, 8, KIND>(a, st);
+  else if (C <= 16) ps_scan_c<M, 16, KIND>(a, st);
+  else if (C <= 24) ps_scan_c<M, 24, KIND>(a, st);
+  else ps_scan_c<M, 32, KIND>(a, st);
+}
+
+template <int KIND>
+static int ps_scan(int mode, const PsScanArgs& a, cudaStream_t st) {
+  if (a.Nw > 1024) return set_err(DDFAN_ERR_UNSUPPORTED, "slice-major prefix sums: line of %d cells", a.Nw);
+  if (a.nlines < 1) return DDFAN_OK;
+  switch (mode) {
+    case SAT_FP32: ps_scan_go<SAT_FP32, KIND>(a, st); break;
+    case SAT_HILO: ps_scan_go<SAT_HILO, KIND>(a, st); break;
+    default: ps_scan_go<SAT_FP64, KIND>(a, st); break;
+  }
+  return ps_check("k_ps_scan");
+}
+
+// Both image tables of the current image (rows from d_x, columns from its transpose).
+static int ps_sat_image(Solver& s, cudaStream_t st) {
+  const Plan& p = *s.P;
+  const size_t V = (size_t)s.XN * s.YN * s.Z;
+  int rc;
+  if ((rc = ps_transpose(s.d_x, s.d_xt, s.Z, s.YN, s.XN, st))) return rc;
+  PsScanArgs a{};
+  a.mask = p.has_mask ? p.d_mask : nullptr;
+  a.XN = s.XN;
+  a.tab = s.d_tabx; a.nlines = s.Z * s.YN; a.N = a.Nw = s.XN; a.src = s.d_x; a.lines_per_slice = s.YN; a.cols = 0;
+  if ((rc = ps_scan<0>(p.mode, a, st))) return rc;
+  a.tab = s.d_taby; a.nlines = s.Z * s.XN; a.N = a.Nw = s.YN; a.src = s.d_xt; a.lines_per_slice = s.XN; a.cols = 1;
+  return ps_scan<0>(p.mode, a, st);
+}
+
+static int ps_fwd(int mode, const PsFwdArgs& a, int cnt, int Z, cudaStream_t st) {
+  dim3 grid((a.U + 247) / 248, cnt, Z);
+  switch (mode) {
+    case SAT_FP32: k_ps_fwd<SAT_FP32><<<grid, 256, 0, st>>>(a); break;
+    case SAT_HILO: k_ps_fwd<SAT_HILO><<<grid, 256, 0, st>>>(a); break;
+    default: k_ps_fwd<SAT_FP64><<<grid, 256, 0, st>>>(a); break;
+  }
+  return ps_check("k_ps_fwd");
+}
+
+static int ps_back(int mode, const PsBackArgs& a, int Z, cudaStream_t st) {
+  dim3 grid((a.XN + 61) / 62, (a.YN + 31) / 32, Z);
+  switch (mode) {
+    case SAT_FP32: k_ps_back_adj<SAT_FP32><<<grid, 256, 0, st>>>(a); break;
+    case SAT_HILO: k_ps_back_adj<SAT_HILO><<<grid, 256, 0, st>>>(a); break;
+    default: k_ps_back_adj<SAT_FP64><<<grid, 256, 0, st>>>(a); break;
+  }
+  return ps_check("k_ps_back_adj");
+}
+
+// Subset k of a slice-major iteration: every slice's own views k, k + nOS, ...
+static int ps_subset(Solver& s, int k, cudaStream_t st) {
+  const Plan& p = *s.P;
+  const int Z = s.Z, U = s.U, c = s.cnt[k];
+  const size_t V = (size_t)s.XN * s.YN * Z;
+  const size_t rows = (size_t)Z * s.cstride;
+  int rc;
+  // geometry of every slice's views of the subset
+  if ((rc = launch_view_geom(p, s.d_pang + (size_t)k * rows, 1, (int)rows, s.d_vg, s.d_fc, s.d_cvd, st)))
+    return rc;
+  // project the current image (AAPM_script/OSSART_AAPM.m:85)
+  {
+    ProfScope ps(KIND_SAT_IMAGE, st);
+    if ((rc = ps_sat_image(s, st))) return rc;
+  }
+  {
+    ProfScope ps(KIND_FWD, st);
+    PsFwdArgs f;
+    f.tabx = s.d_tabx; f.taby = s.d_taby;
+    f.vg = s.d_vg; f.fc = s.d_fc; f.cvd = s.d_cvd; f.out = s.d_ax;
+    f.cstride = s.cstride; f.U = U; f.XN = s.XN; f.YN = s.YN; f.dx = (float)p.dx;
+    if ((rc = ps_fwd(p.mode, f, c, Z, st))) return rc;
+  }
+  // residual (y - A x) / rowSum, weighted, into channel prefix sums (:86-88)
+  {
+    ProfScope ps(KIND_SAT_SINO, st);
+    PsScanArgs r{};
+    r.tab = s.d_sq; r.nlines = Z * c; r.N = U; r.Nw = U + 1;
+    r.y = s.d_y; r.ax = s.d_ax; r.rows = s.d_rows; r.wgt = s.d_cvd; r.wscale = 1.f;
+    r.cnt = c; r.cstride = s.cstride; r.P = s.PNall; r.roff = s.off[k]; r.ksub = k; r.nOS = s.nsub;
+    if ((rc = ps_scan<1>(p.mode, r, st))) return rc;
+  }
+  // exact-adjoint backprojection, divide by colSum, add, optional clamp (:91-97)
+  ProfScope ps(KIND_BACK_A, st);
+  PsBackArgs b{};
+  b.sq = s.d_sq; b.vg = s.d_vg; b.fc = s.d_fc;
+  b.tb = p.d_tb; b.lut = p.d_lut; b.t0 = p.t0; b.invdt = p.invdt; b.dirt = p.dirt; b.M = p.M;
+  b.cnt = c; b.cstride = s.cstride; b.U = U; b.XN = s.XN; b.YN = s.YN;
+  b.ocx = p.ocx; b.ocy = p.ocy; b.dx = p.dx;
+  b.x = s.d_x; b.colsum = s.d_cols + (size_t)k * s.XN * s.YN; b.nonneg = s.nonneg;
+  b.mask = p.has_mask ? p.d_mask : nullptr;
+  return ps_back(p.mode, b, Z, st);
+}
+
 // One OS-SART iteration (AAPM_script/OSSART_AAPM.m:79-115) on stream st.
 static int solver_iteration(Solver& s, cudaStream_t st) {
   Plan& p = *s.P;
   int rc, n = 0;
   const bool adj = s.back_mode == DDFAN_BACK_ADJ;
-  for (int k = 0; k < s.nsub; ++k) {
+  for (int k = 0; k < s.nsub && s.ps; ++k) {
+    if ((rc = ps_subset(s, k, st))) return rc;
+    n += 7;
+  }
+  for (int k = 0; k < s.nsub && !s.ps; ++k) {
     const int o = s.off[k], c = s.cnt[k];
     BackEpi e{};
     e.out = s.d_x; e.xin = s.d_x; e.colsum = s.d_cols + (size_t)k * s.XN * s.YN;
@@ -309,8 +450,10 @@ static int solver_iteration(Solver& s, cudaStream_t st) {
   return DDFAN_OK;
 }
 
-// The image in the caller's slice order (windowed solver), after iterations.
+// The image in the caller's layout and slice order (windowed and slice-major
+// solvers), after iterations.
 static int solver_publish(Solver& s, cudaStream_t st) {
+  if (s.ps) return ps_transpose(s.d_x, s.d_xu, 1, s.Z, s.XN * s.YN, st);
   if (!s.win) return DDFAN_OK;
   return gather_slices(s.d_x, s.Zi, s.d_xu, s.Z, s.d_inv, (size_t)s.XN * s.YN, st);
 }
@@ -507,6 +650,16 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
   angle_windows(hangs, PNall, SLN, G, woff);
   s.win = false;
   for (int z = 1; z < SLN; ++z) s.win = s.win || woff[z] != woff[0];
+  // Per-slice angle lists go to the slice-major path (exact adjoint only);
+  // DDFAN_PER_SLICE=windowed keeps them on the windowed path, =slices sends
+  // shared lists to the slice-major path too.
+  {
+    const char* pv = getenv("DDFAN_PER_SLICE");
+    const bool want_win = pv && !std::strcmp(pv, "windowed");
+    const bool want_ps = pv && !std::strcmp(pv, "slices");
+    s.ps = back_mode == DDFAN_BACK_ADJ && (want_ps || (s.win && !want_win));
+    if (s.ps) s.win = false;
+  }
   WinLayout W;
   if (s.win) {
     // z-tile width: views per tile x blocks per tile x relative cost of a block
@@ -531,13 +684,17 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
   PlanDesc d{x0, y0, DNU, xds, yds, detCntIdx, imgXCenter, imgYCenter, XN, YN, dx, mask, s.Zi, std::max(PNmax, 1),
              sat_mode, device};
   if (s.win) d.zl_force = W.ZL;
-  int rc = plan_create(&s.P, d);
+  // the slice-major path uses the plan's geometry, mask and bracket tables only
+  PlanDesc dp = d;
+  if (s.ps) dp.SLN = dp.PNmax = 1;
+  int rc = plan_create(&s.P, dp);
   if (rc) return rc;
   s.bytes = s.P->bytes;
   DeviceGuard g(device);
   const size_t V = (size_t)XN * YN * s.Zi;
-  const size_t R = s.win ? (size_t)numOfOS * s.Mc : P;  // geometry rows
-  const size_t nord = s.win ? (size_t)std::max<long long>(W.cost, 1) : P;
+  if (s.ps) s.cstride = PNsub;
+  const size_t R = s.win ? (size_t)numOfOS * s.Mc : (s.ps ? (size_t)SLN * s.cstride : P);  // geometry rows
+  const size_t nord = s.win ? (size_t)std::max<long long>(W.cost, 1) : (s.ps ? 1 : P);
   DDFAN_CK(cudaStreamCreateWithFlags(&s.own, cudaStreamNonBlocking));
   DDFAN_CK(cudaEventCreateWithFlags(&s.last_use, cudaEventDisableTiming));
   if ((rc = salloc(s, &s.d_vg, R)) || (rc = salloc(s, &s.d_fc, R * (DNU + 1))) ||
@@ -549,7 +706,22 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
     return rc;
   cudaStream_t st = s.own;
   DDFAN_CK(cudaMemcpyAsync(s.d_yview, yview.data(), sizeof(int) * P, cudaMemcpyHostToDevice, st));
-  if (!s.win) {
+  if (s.ps) {
+    // angles of view k + m * numOfOS of every slice z, per subset k: row (k, z, m)
+    std::vector<float> pang((size_t)numOfOS * SLN * s.cstride, 0.f);
+    for (int k = 0; k < numOfOS; ++k)
+      for (int z = 0; z < SLN; ++z)
+        for (int m = 0; m < s.cnt[k]; ++m)
+          pang[((size_t)k * SLN + z) * s.cstride + m] = hangs[(size_t)(k + m * numOfOS) * SLN + z];
+    const size_t CF = sat_mode == SAT_FP32 ? 2 : 4;  // floats per slice-major cell
+    if ((rc = salloc(s, &s.d_pang, pang.size())) || (rc = salloc(s, &s.d_xt, V)) ||
+        (rc = salloc(s, &s.d_tabx, CF * V)) || (rc = salloc(s, &s.d_taby, CF * V)) ||
+        (rc = salloc(s, &s.d_sq, CF * R * (DNU + 1))) || (rc = salloc(s, &s.d_xu, V)) ||
+        (rc = salloc(s, &s.d_stage, P * DNU * SLN)))
+      return rc;
+    DDFAN_CK(cudaMemcpyAsync(s.d_pang, pang.data(), sizeof(float) * pang.size(), cudaMemcpyHostToDevice, st));
+    DDFAN_CK(cudaStreamSynchronize(st));
+  } else if (!s.win) {
     // per-view tables for every view, in subset order; per subset the views
     // of one orientation together (one image table at a time stays hot in
     // L2; the exact adjoint visits each orientation in turn)
@@ -668,7 +840,16 @@ DDFAN_API int ddfan_ossart_set_sinogram(ddfan_ossart* h, const float* proj, int 
   DeviceGuard g(s->device);
   const size_t n = (size_t)s->PNall * s->U * s->Z;
   cudaStream_t st = (cudaStream_t)stream;
-  if (!s->win) {
+  if (s->ps) {
+    // slice-major [Z][PNall][U]
+    const float* src = proj;
+    if (!is_device) {
+      DDFAN_CK(cudaMemcpyAsync(s->d_stage, proj, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+      src = s->d_stage;
+    }
+    int rc = ps_transpose(src, s->d_y, 1, (long long)s->PNall * s->U, s->Z, st);
+    if (rc) return rc;
+  } else if (!s->win) {
     DDFAN_CK(cudaMemcpyAsync(s->d_y, proj, sizeof(float) * n,
                              is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
   } else {
@@ -691,7 +872,12 @@ DDFAN_API int ddfan_ossart_set_image(ddfan_ossart* h, const float* img, int is_d
   DeviceGuard g(s->device);
   const size_t n = (size_t)s->XN * s->YN * s->Z;
   cudaStream_t st = (cudaStream_t)stream;
-  if (!s->win) {
+  if (s->ps) {
+    DDFAN_CK(cudaMemcpyAsync(s->d_xu, img, sizeof(float) * n,
+                             is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    int rc = ps_transpose(s->d_xu, s->d_x, 1, (long long)s->XN * s->YN, s->Z, st);
+    if (rc) return rc;
+  } else if (!s->win) {
     DDFAN_CK(cudaMemcpyAsync(s->d_x, img, sizeof(float) * n,
                              is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
   } else {
@@ -750,7 +936,7 @@ DDFAN_API int ddfan_ossart_get_image(ddfan_ossart* h, float* img, int is_device,
   DeviceGuard g(s->device);
   const size_t n = (size_t)s->XN * s->YN * s->Z;
   cudaStream_t st = (cudaStream_t)stream;
-  DDFAN_CK(cudaMemcpyAsync(img, s->win ? s->d_xu : s->d_x, sizeof(float) * n,
+  DDFAN_CK(cudaMemcpyAsync(img, (s->win || s->ps) ? s->d_xu : s->d_x, sizeof(float) * n,
                            is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
   cudaEventRecord(s->last_use, st);
   if (!is_device) DDFAN_CK(cudaStreamSynchronize(st));
@@ -785,13 +971,13 @@ DDFAN_API int ddfan_ossart_profile(ddfan_ossart* h, int numOfIter, void* stream,
 
 DDFAN_API float* ddfan_ossart_image_ptr(ddfan_ossart* h) {
   Solver* s = reinterpret_cast<Solver*>(h);
-  return s ? (s->win ? s->d_xu : s->d_x) : nullptr;
+  return s ? ((s->win || s->ps) ? s->d_xu : s->d_x) : nullptr;
 }
 
 DDFAN_API int ddfan_ossart_launches_per_iter(const ddfan_ossart* h) {
   const Solver* s = reinterpret_cast<const Solver*>(h);
   if (!s) return 0;
-  return s->nsub * (s->back_mode == DDFAN_BACK_ADJ ? 5 : 4) + (s->useFISTA ? 2 : 0);
+  return s->nsub * (s->ps ? 7 : (s->back_mode == DDFAN_BACK_ADJ ? 5 : 4)) + (s->useFISTA ? 2 : 0);
 }
 
 DDFAN_API int ddfan_OSSART_AAPM(float x0, float y0, int DNU, const float* xds, const float* yds,
