@@ -371,6 +371,9 @@ struct PsBackArgs {
   const uint8_t* mask;
 };
 
+// rows of pixels per warp in k_ps_back_adj (8 warps: 2 across x, 4 down y)
+constexpr int kPsBackRows = 8;
+
 // Exact transpose of k_ps_fwd, both view orientations in one pass.  Warp =
 // 31 consecutive pixels of a row (lanes 0..30) x R rows of one slice; it
 // loops over the slice's views of the subset.  A view integrated along x
@@ -383,10 +386,11 @@ struct PsBackArgs {
 // by the edge's fan tangent (lookup table + correction steps, as k_back_adj)
 // and then walks: it keeps c_b and c_{b+1} at its current line and steps b
 // when the next edge crosses a boundary -- boundary rays do not cross inside
-// the image, so s c_b(li) increases with b on every line (s = the view's sgn).
+// the image, so s c_b(li) increases with b on every line (s = the view's sgn);
+// the walk runs on s-scaled positions.
 template <int M>
 __global__ void __launch_bounds__(256) k_ps_back_adj(PsBackArgs a) {
-  constexpr int R = 8, PX = 31;
+  constexpr int R = kPsBackRows, PX = 31;
   constexpr int TBMAX = 1024, LUTMAX = 4096;
   using Cell = typename PsCell<M>::T;
   __shared__ float s_tb[TBMAX];
@@ -434,24 +438,29 @@ __global__ void __launch_bounds__(256) k_ps_back_adj(PsBackArgs a) {
         while (b > 0 && s_tb[b] > t && guard++ < 128) --b;
       }
     }
-    double2 f0 = __ldg(fcr + b), f1 = __ldg(fcr + b + 1);
-    double c0 = fma(di, f0.x, f0.y), c1 = fma(di, f1.x, f1.y);
     const double s = (double)sgn;
+    auto line_at = [&](int bb) {  // s-scaled boundary line (slope, offset)
+      const double2 f = __ldg(fcr + bb);
+      return make_double2(s * f.x, s * f.y);
+    };
+    dk *= s;
+    double2 f0 = line_at(b), f1 = line_at(b + 1);
+    double c0 = fma(di, f0.x, f0.y), c1 = fma(di, f1.x, f1.y);
     // Q at the current edge after moving the bracket onto it
     auto sample = [&]() {
       int guard = 0;
-      while (b < U - 1 && s * (dk - c1) >= 0.0 && guard++ < 1024) {
+      while (b < U - 1 && dk >= c1 && guard++ < 1024) {
         ++b;
         f0 = f1;
         c0 = c1;
-        f1 = __ldg(fcr + b + 1);
+        f1 = line_at(b + 1);
         c1 = fma(di, f1.x, f1.y);
       }
-      while (b > 0 && s * (dk - c0) < 0.0 && guard++ < 2048) {
+      while (b > 0 && dk < c0 && guard++ < 2048) {
         --b;
         f1 = f0;
         c1 = c0;
-        f0 = __ldg(fcr + b);
+        f0 = line_at(b);
         c0 = fma(di, f0.x, f0.y);
       }
       const float frac = fminf(fmaxf((float)(dk - c0) * rcp_approx((float)(c1 - c0)), 0.f), 1.f);
@@ -464,7 +473,7 @@ __global__ void __launch_bounds__(256) k_ps_back_adj(PsBackArgs a) {
       PhiS<M> prev = sample();
 #pragma unroll
       for (int i = 0; i < R; ++i) {
-        dk += 1.0;
+        dk += s;
         const PhiS<M> cur = sample();
         acc[i] = fmaf(sgn, cur.diff(prev), acc[i]);
         prev = cur;

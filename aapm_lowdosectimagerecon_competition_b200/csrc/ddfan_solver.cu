@@ -343,7 +343,7 @@ static int ps_fwd(int mode, const PsFwdArgs& a, int cnt, int Z, cudaStream_t st)
 }
 
 static int ps_back(int mode, const PsBackArgs& a, int Z, cudaStream_t st) {
-  dim3 grid((a.XN + 61) / 62, (a.YN + 31) / 32, Z);
+  dim3 grid((a.XN + 61) / 62, (a.YN + 4 * kPsBackRows - 1) / (4 * kPsBackRows), Z);
   switch (mode) {
     case SAT_FP32: k_ps_back_adj<SAT_FP32><<<grid, 256, 0, st>>>(a); break;
     case SAT_HILO: k_ps_back_adj<SAT_HILO><<<grid, 256, 0, st>>>(a); break;
@@ -617,6 +617,10 @@ static int solver_weights(Solver& s, const PlanDesc& d, const std::vector<float>
   return DDFAN_OK;
 }
 
+// Iteration time of the slice-major path over the shared-list path, measured
+// at 512 x 512 x 128 with 24 subsets of 96 views.
+static constexpr double kSliceMajorCost = 2.9;
+
 static int solver_create(Solver** out, float x0, float y0, int DNU, const float* xds, const float* yds,
                          float detCntIdx, float imgXCenter, float imgYCenter, const float* hangs,
                          int PNall, int XN, int YN, int SLN, float dx, const uint8_t* mask,
@@ -650,17 +654,8 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
   angle_windows(hangs, PNall, SLN, G, woff);
   s.win = false;
   for (int z = 1; z < SLN; ++z) s.win = s.win || woff[z] != woff[0];
-  // Per-slice angle lists go to the slice-major path (exact adjoint only);
-  // DDFAN_PER_SLICE=windowed keeps them on the windowed path, =slices sends
-  // shared lists to the slice-major path too.
-  {
-    const char* pv = getenv("DDFAN_PER_SLICE");
-    const bool want_win = pv && !std::strcmp(pv, "windowed");
-    const bool want_ps = pv && !std::strcmp(pv, "slices");
-    s.ps = back_mode == DDFAN_BACK_ADJ && (want_ps || (s.win && !want_win));
-    if (s.ps) s.win = false;
-  }
   WinLayout W;
+  double win_cost = 0.0;  // windowed projector work relative to shared angle lists
   if (s.win) {
     // z-tile width: views per tile x blocks per tile x relative cost of a block
     // at that width (the projector cost model of pow2_zl)
@@ -676,6 +671,20 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
         W = t;
       }
     }
+    win_cost = best / ((double)PNall * ((SLN + 3) / 4));
+  }
+  // Per-slice angle lists whose windows share little go to the slice-major
+  // path (exact adjoint only), which costs about kSliceMajorCost times the
+  // shared-list iteration whatever the lists; DDFAN_PER_SLICE=windowed or
+  // =slices overrides the choice (=slices also for shared lists).
+  {
+    const char* pv = getenv("DDFAN_PER_SLICE");
+    const bool want_win = pv && !std::strcmp(pv, "windowed");
+    const bool want_ps = pv && !std::strcmp(pv, "slices");
+    s.ps = back_mode == DDFAN_BACK_ADJ && (want_ps || (s.win && !want_win && win_cost > kSliceMajorCost));
+    if (s.ps) s.win = false;
+  }
+  if (s.win) {
     s.Zi = W.Zi; s.nzt = W.nzt; s.Mc = W.Mc; s.perm = W.perm; s.maxcnt = W.maxcnt;
   } else {
     s.Zi = SLN;
