@@ -98,6 +98,12 @@ template <> struct AccS<SAT_FP32> {
   __device__ __forceinline__ static float2 cell(const float* buf, int NB, int i, float v) {
     return make_float2(buf[i], v);
   }
+  __device__ __forceinline__ AccS bcast(int src) const {
+    AccS r;
+    r.s = __shfl_sync(0xffffffffu, s, src);
+    return r;
+  }
+  __device__ __forceinline__ float2 cell(float v) const { return make_float2(s, v); }
 };
 
 template <> struct AccS<SAT_HILO> {
@@ -130,6 +136,16 @@ template <> struct AccS<SAT_HILO> {
   __device__ __forceinline__ static float4 cell(const float* buf, int NB, int i, float v) {
     return make_float4(buf[i], buf[NB + i], v, 0.f);
   }
+  __device__ __forceinline__ AccS bcast(int src) const {
+    AccS r;
+    r.hi = __shfl_sync(0xffffffffu, hi, src);
+    r.lo = __shfl_sync(0xffffffffu, lo, src);
+    return r;
+  }
+  __device__ __forceinline__ float4 cell(float v) const {
+    const float s = __fadd_rn(hi, lo);
+    return make_float4(s, __fsub_rn(lo, __fsub_rn(s, hi)), v, 0.f);
+  }
 };
 
 template <> struct AccS<SAT_FP64> {
@@ -148,6 +164,14 @@ template <> struct AccS<SAT_FP64> {
   }
   __device__ __forceinline__ static float4 cell(const float* buf, int NB, int i, float v) {
     return make_float4(buf[i], buf[NB + i], v, 0.f);
+  }
+  __device__ __forceinline__ AccS bcast(int src) const {
+    AccS r;
+    r.s = __shfl_sync(0xffffffffu, s, src);
+    return r;
+  }
+  __device__ __forceinline__ float4 cell(float v) const {
+    return make_float4(__int_as_float(__double2loint(s)), __int_as_float(__double2hiint(s)), v, 0.f);
   }
 };
 
@@ -196,7 +220,8 @@ static __global__ void __launch_bounds__(256) k_ps_transpose(const float* __rest
 // or columns) or the OS-SART residual of one (slice, view) of a subset.
 struct PsScanArgs {
   void* tab;            // cells (PsCell<M>::T), line t at [t * Nw, t * Nw + Nw)
-  int nlines, N, Nw;    // lines, values per line, cells per line (Nw >= N; cells past N hold the total)
+  int nlines, N, Nw;    // lines, values per line, cells per line (Nw >= N + pad; cells past the values hold the total)
+  int pad;              // zero cells before the values (image tables: 1, the guard cell of clamped samples)
   // image: src [nlines][N] (slice-major, lines of a slice contiguous); mask [YN][XN]
   const float* src;
   const uint8_t* mask;
@@ -235,9 +260,10 @@ __device__ __forceinline__ float ps_value(const PsScanArgs& a, int line, int k) 
 }
 
 // One warp per line, WPC warps per CTA.  Lane L owns the chunk
-// [L*C, L*C + C) of the line; values go through shared memory both ways so
-// that global reads and cell writes are coalesced.  Chunk sums are combined
-// by a warp-shuffle exclusive scan.
+// [L*C, L*C + C) of the line's N values (32 C >= N); values go through shared
+// memory both ways so that global reads and cell writes are coalesced.  Chunk
+// sums are combined by a warp-shuffle exclusive scan.  Cells: pad zero cells,
+// the N value cells, then cells holding the total up to Nw.
 template <int M, int C, int KIND>
 __global__ void __launch_bounds__(128) k_ps_scan(PsScanArgs a) {
   constexpr int WPC = C > 24 ? 2 : 4;
@@ -256,6 +282,7 @@ __global__ void __launch_bounds__(128) k_ps_scan(PsScanArgs a) {
     tline = z * a.cstride + (line - z * a.cnt);
   }
   Cell* out = reinterpret_cast<Cell*>(a.tab) + (size_t)tline * a.Nw;
+  Cell* vout = out + a.pad;
   auto slot = [](int e) { return (e / C) * (C + 1) + e % C; };
   for (int e = lane; e < 32 * C; e += 32) vbuf[slot(e)] = ps_value<KIND>(a, line, e);
   __syncwarp();
@@ -280,15 +307,22 @@ __global__ void __launch_bounds__(128) k_ps_scan(PsScanArgs a) {
     run.put(buf, NB, lane * (C + 1) + j);
     run.add(v[j]);
   }
+  const AccS<M> total = run.bcast(31);
   __syncwarp();
-  for (int e = lane; e < a.Nw; e += 32) out[e] = AccS<M>::cell(buf, NB, slot(e), vbuf[slot(e)]);
+  for (int e = lane; e < a.N; e += 32) vout[e] = AccS<M>::cell(buf, NB, slot(e), vbuf[slot(e)]);
+  if (lane < a.pad) {
+    AccS<M> zero;
+    zero.zero();
+    out[lane] = zero.cell(0.f);
+  }
+  for (int e = a.N + a.pad + lane; e < a.Nw; e += 32) out[e] = total.cell(0.f);
 }
 
 // ---------------------------------------------------------------- forward
 
 struct PsFwdArgs {
-  const void* tabx;   // image rows [Z][YN][XN] cells (y-major views)
-  const void* taby;   // image columns [Z][XN][YN] cells (x-major views)
+  const void* tabx;   // image rows [Z][YN][XN + 2] cells (y-major views), guard cell first and last
+  const void* taby;   // image columns [Z][XN][YN + 2] cells (x-major views)
   const ViewGeom* vg;   // rows z * cstride + m
   const double2* fc;    // [rows][U+1] boundary lines
   const float* cvd;     // [rows][U]
@@ -304,7 +338,9 @@ struct PsFwdArgs {
 // line, summing chunks of 16 lines into a fresh partial as k_fwd does.  The
 // boundary position c_b(ii) = ii F + C runs in 32.32 fixed point from the FP64
 // line (error below 1e-7 cells over 1024 lines); the footprint length
-// (c_{b+1} - c_b) dx is linear in ii and runs in FP32.
+// (c_{b+1} - c_b) dx is linear in ii and runs in FP32.  Positions outside the
+// line clamp to its guard cells (prefix sum 0 before, the total after, value
+// 0), which reproduces k_fwd's clamp of c to [0, N].
 template <int M>
 __global__ void __launch_bounds__(256) k_ps_fwd(PsFwdArgs a) {
   constexpr int CC = 16, CPW = 31;
@@ -317,7 +353,8 @@ __global__ void __launch_bounds__(256) k_ps_fwd(PsFwdArgs a) {
   const int b = bw + lane;
   const bool xm = a.vg[r].xmajor != 0;
   const int nl = xm ? a.XN : a.YN, N = xm ? a.YN : a.XN;
-  const Cell* line = reinterpret_cast<const Cell*>(xm ? a.taby : a.tabx) + (size_t)z * nl * N;
+  const int Nw = N + 2;
+  const Cell* line = reinterpret_cast<const Cell*>(xm ? a.taby : a.tabx) + (size_t)z * nl * Nw;
   const double2 f0 = __ldg(a.fc + r * (a.U + 1) + min(b, a.U));
   const double2 f1 = __ldg(a.fc + r * (a.U + 1) + min(b + 1, a.U));
   const double two32 = 4294967296.0;
@@ -332,18 +369,15 @@ __global__ void __launch_bounds__(256) k_ps_fwd(PsFwdArgs a) {
     float part = 0.f;
 #pragma unroll 4
     for (int col = 0; col < ncol; ++col) {
-      const int hi = (int)(cf >> 32);
-      float f = __int_as_float(0x3f800000 | ((unsigned)cf >> 9)) - 1.f;
-      int i0 = hi;
-      if (hi < 0) { i0 = 0; f = 0.f; }
-      if (hi >= N) { i0 = N - 1; f = 1.f; }
+      const int i0 = min(max((int)(cf >> 32), -1), N) + 1;
+      const float f = __int_as_float(0x3f800000 | ((unsigned)cf >> 9)) - 1.f;
       PhiS<M> cur;
       cur.load(line + i0, f);
       const PhiS<M> nxt = cur.down();
       part = fmaf(nxt.diff(cur), rcp_approx(fmaf(fi, lF, lC)), part);
       cf += dcf;
       fi += 1.f;
-      line += N;
+      line += Nw;
     }
     acc += part;
   }
@@ -382,27 +416,25 @@ constexpr int kPsBackRows = 8;
 // and differences neighbouring lanes.  The sample at a pixel edge (line li,
 // edge ck) is the weighted channel prefix sum Q at the edge's fractional
 // boundary index b + (ck - c_b(li)) / (c_{b+1}(li) - c_b(li)), c_b the FP64
-// boundary lines of the forward.  Each lane brackets its first edge of a view
-// by the edge's fan tangent (lookup table + correction steps, as k_back_adj)
+// boundary lines of the forward.  Each lane guesses the bracket of its first
+// edge of a view from the edge's fan tangent (the lookup table of k_back_adj)
 // and then walks: it keeps c_b and c_{b+1} at its current line and steps b
-// when the next edge crosses a boundary -- boundary rays do not cross inside
+// until the edge lies between them -- boundary rays do not cross inside
 // the image, so s c_b(li) increases with b on every line (s = the view's sgn);
 // the walk runs on s-scaled positions.
 template <int M>
 __global__ void __launch_bounds__(256) k_ps_back_adj(PsBackArgs a) {
   constexpr int R = kPsBackRows, PX = 31;
-  constexpr int TBMAX = 1024, LUTMAX = 4096;
+  constexpr int LUTMAX = 4096;
   using Cell = typename PsCell<M>::T;
-  __shared__ float s_tb[TBMAX];
   __shared__ uint16_t s_lut[LUTMAX];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  for (int i = tid; i <= a.U; i += 256) s_tb[i] = a.tb[i];
   for (int i = tid; i < a.M; i += 256) s_lut[i] = a.lut[i];
   __syncthreads();
   const int z = blockIdx.z;
   const int x0 = (blockIdx.x * 2 + (w & 1)) * PX, y0 = (blockIdx.y * 4 + (w >> 1)) * R;
   if (x0 >= a.XN || y0 >= a.YN) return;  // uniform per warp; no barrier below
-  const float tfirst = s_tb[0], tlast = s_tb[a.U];
+  const float tfirst = __ldg(a.tb), tlast = __ldg(a.tb + a.U);
   const int U = a.U;
   const size_t rowQ = (size_t)(U + 1);
   float acc[R];
@@ -431,11 +463,9 @@ __global__ void __launch_bounds__(256) k_ps_back_adj(PsBackArgs a) {
       } else if (t >= tlast) {
         b = U - 1;
       } else {
+        // a guess within a boundary or two; the walk below makes it exact
         const float mf = fminf(fmaxf((t - a.t0) * a.invdt, 0.f), (float)(a.M - 1));
         b = s_lut[(int)mf];
-        int guard = 0;
-        while (b < U - 1 && s_tb[b + 1] <= t && guard++ < 64) ++b;
-        while (b > 0 && s_tb[b] > t && guard++ < 128) --b;
       }
     }
     const double s = (double)sgn;
@@ -447,16 +477,16 @@ __global__ void __launch_bounds__(256) k_ps_back_adj(PsBackArgs a) {
     double2 f0 = line_at(b), f1 = line_at(b + 1);
     double c0 = fma(di, f0.x, f0.y), c1 = fma(di, f1.x, f1.y);
     // Q at the current edge after moving the bracket onto it
+    // (each loop moves b towards one end of [0, U - 1] and stops there)
     auto sample = [&]() {
-      int guard = 0;
-      while (b < U - 1 && dk >= c1 && guard++ < 1024) {
+      while (b < U - 1 && dk >= c1) {
         ++b;
         f0 = f1;
         c0 = c1;
         f1 = line_at(b + 1);
         c1 = fma(di, f1.x, f1.y);
       }
-      while (b > 0 && dk < c0 && guard++ < 2048) {
+      while (b > 0 && dk < c0) {
         --b;
         f1 = f0;
         c1 = c0;

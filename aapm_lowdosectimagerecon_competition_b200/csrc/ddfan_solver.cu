@@ -298,7 +298,7 @@ static void ps_scan_c(const PsScanArgs& a, cudaStream_t st) {
 
 template <int M, int KIND>
 static void ps_scan_go(const PsScanArgs& a, cudaStream_t st) {
-  const int C = (a.Nw + 31) / 32;
+  const int C = (a.N + 31) / 32;
   if (C <= 8) ps_scan_c<M, 8, KIND>(a, st);
   else if (C <= 16) ps_scan_c<M, 16, KIND>(a, st);
   else if (C <= 24) ps_scan_c<M, 24, KIND>(a, st);
@@ -307,7 +307,8 @@ static void ps_scan_go(const PsScanArgs& a, cudaStream_t st) {
 
 template <int KIND>
 static int ps_scan(int mode, const PsScanArgs& a, cudaStream_t st) {
-  if (a.Nw > 1024) return set_err(DDFAN_ERR_UNSUPPORTED, "slice-major prefix sums: line of %d cells", a.Nw);
+  if (a.N > 1024 || a.Nw < a.N + a.pad)
+    return set_err(DDFAN_ERR_UNSUPPORTED, "slice-major prefix sums: line of %d cells", a.Nw);
   if (a.nlines < 1) return DDFAN_OK;
   switch (mode) {
     case SAT_FP32: ps_scan_go<SAT_FP32, KIND>(a, st); break;
@@ -326,9 +327,12 @@ static int ps_sat_image(Solver& s, cudaStream_t st) {
   PsScanArgs a{};
   a.mask = p.has_mask ? p.d_mask : nullptr;
   a.XN = s.XN;
-  a.tab = s.d_tabx; a.nlines = s.Z * s.YN; a.N = a.Nw = s.XN; a.src = s.d_x; a.lines_per_slice = s.YN; a.cols = 0;
+  a.pad = 1;  // guard cells: one before the line, one after (the total)
+  a.tab = s.d_tabx; a.nlines = s.Z * s.YN; a.N = s.XN; a.Nw = s.XN + 2; a.src = s.d_x; a.lines_per_slice = s.YN;
+  a.cols = 0;
   if ((rc = ps_scan<0>(p.mode, a, st))) return rc;
-  a.tab = s.d_taby; a.nlines = s.Z * s.XN; a.N = a.Nw = s.YN; a.src = s.d_xt; a.lines_per_slice = s.XN; a.cols = 1;
+  a.tab = s.d_taby; a.nlines = s.Z * s.XN; a.N = s.YN; a.Nw = s.YN + 2; a.src = s.d_xt; a.lines_per_slice = s.XN;
+  a.cols = 1;
   return ps_scan<0>(p.mode, a, st);
 }
 
@@ -617,9 +621,12 @@ static int solver_weights(Solver& s, const PlanDesc& d, const std::vector<float>
   return DDFAN_OK;
 }
 
-// Iteration time of the slice-major path over the shared-list path, measured
-// at 512 x 512 x 128 with 24 subsets of 96 views.
-static constexpr double kSliceMajorCost = 2.9;
+// The windowed cost (projector work over that of shared lists) above which
+// the slice-major path is faster.  Measured at 512 x 512 x 128, 24 subsets of
+// 96 views: slice-major iterations take 2.05x the shared-list time whatever
+// the lists; windowed ones 2.13x at a modelled cost of 1.76 (slices 36 raw
+// views apart) and 13.5x at 13.3 (86.07 apart).
+static constexpr double kSliceMajorCost = 1.7;
 
 static int solver_create(Solver** out, float x0, float y0, int DNU, const float* xds, const float* yds,
                          float detCntIdx, float imgXCenter, float imgYCenter, const float* hangs,
@@ -723,8 +730,9 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
         for (int m = 0; m < s.cnt[k]; ++m)
           pang[((size_t)k * SLN + z) * s.cstride + m] = hangs[(size_t)(k + m * numOfOS) * SLN + z];
     const size_t CF = sat_mode == SAT_FP32 ? 2 : 4;  // floats per slice-major cell
+    const size_t VG = (size_t)(XN + 2) * (YN + 2) * SLN;  // cells of a table with guard cells
     if ((rc = salloc(s, &s.d_pang, pang.size())) || (rc = salloc(s, &s.d_xt, V)) ||
-        (rc = salloc(s, &s.d_tabx, CF * V)) || (rc = salloc(s, &s.d_taby, CF * V)) ||
+        (rc = salloc(s, &s.d_tabx, CF * VG)) || (rc = salloc(s, &s.d_taby, CF * VG)) ||
         (rc = salloc(s, &s.d_sq, CF * R * (DNU + 1))) || (rc = salloc(s, &s.d_xu, V)) ||
         (rc = salloc(s, &s.d_stage, P * DNU * SLN)))
       return rc;
