@@ -16,6 +16,7 @@
 #include "ddfan.h"
 #include "ddfan_kernels.cuh"
 #include "ddfan_plan.h"
+#include "ddfan_ps.h"
 
 namespace ddfan {
 
@@ -175,7 +176,8 @@ void plan_free(Plan* P) {
     if (P->last_use) cudaStreamWaitEvent(P->alloc_stream, P->last_use, 0);
     void* ptrs[] = {P->d_bx, P->d_by, P->d_xd, P->d_yd, P->d_mask, P->d_tb, P->d_lut, P->d_satx,
                     P->d_saty, P->d_satq, P->d_vg, P->d_fc, P->d_cvd, P->d_tmp, P->d_angs,
-                    P->d_order, P->d_counts};
+                    P->d_order, P->d_counts, P->ps_ang, P->ps_vg, P->ps_fc, P->ps_cvd, P->ps_img,
+                    P->ps_imgt, P->ps_sino, P->ps_tabx, P->ps_taby, P->ps_sq};
     for (void* q : ptrs) dev_free(q, P->alloc_stream);
     cudaStreamDestroy(P->alloc_stream);
   }
@@ -662,6 +664,131 @@ static int for_angle_groups(Plan& p, const float* h_angs, int PN, F&& fn, cudaSt
   return DDFAN_OK;
 }
 
+// ------------------------------------------------------------------ per-slice lists
+
+// Slices the grouped path computes for these groups: every contiguous run of
+// a group's slices costs the whole z-tiles that hold it.
+static long long grouped_slices(const Plan& p, const std::vector<std::vector<int>>& groups) {
+  const int tile = 4 * p.ZL;
+  long long n = 0;
+  for (auto& g : groups) {
+    size_t i = 0;
+    while (i < g.size()) {
+      size_t j = i + 1;
+      while (j < g.size() && g[j] == g[j - 1] + 1) ++j;
+      n += (long long)((g[j - 1] + tile) / tile - g[i] / tile) * tile;
+      i = j;
+    }
+  }
+  return n;
+}
+
+// The slice-major kernels cost about twice the shared-list work per slice.
+static bool use_slice_major(const Plan& p, const std::vector<std::vector<int>>& groups, int PN) {
+  return groups.size() > 1 && PN <= 65535 && grouped_slices(p, groups) > 2LL * p.Z;
+}
+
+static int ps_alloc(Plan& p) {
+  if (p.ps_tabx) return DDFAN_OK;
+  const size_t Z = (size_t)p.Z, R = Z * p.PNmax, U = (size_t)p.U;
+  const size_t V = (size_t)p.XN * p.YN * Z, VG = (size_t)(p.XN + 2) * (p.YN + 2) * Z;
+  const size_t CF = p.mode == SAT_FP32 ? 2 : 4;  // floats per slice-major cell
+  size_t& B = p.bytes;
+  cudaStream_t as = p.alloc_stream;
+  int rc;
+  if ((rc = dalloc(&p.ps_ang, R, &B, as)) || (rc = dalloc(&p.ps_vg, R, &B, as)) ||
+      (rc = dalloc(&p.ps_fc, R * (U + 1), &B, as)) || (rc = dalloc(&p.ps_cvd, R * U, &B, as)) ||
+      (rc = dalloc(&p.ps_img, V, &B, as)) || (rc = dalloc(&p.ps_imgt, V, &B, as)) ||
+      (rc = dalloc(&p.ps_sino, R * U, &B, as)) || (rc = dalloc(&p.ps_tabx, CF * VG, &B, as)) ||
+      (rc = dalloc(&p.ps_taby, CF * VG, &B, as)) || (rc = dalloc(&p.ps_sq, CF * R * (U + 1), &B, as)))
+    return rc;
+  // the allocations complete before any stream uses them
+  cudaError_t e = cudaStreamSynchronize(as);
+  if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "slice-major buffers: %s", cudaGetErrorString(e));
+  return DDFAN_OK;
+}
+
+// geometry rows (z, m) of angle list d_angs [PN][Z]
+static int ps_geometry(Plan& p, const float* d_angs, int PN, cudaStream_t st) {
+  int rc = ps_transpose(d_angs, p.ps_ang, 1, PN, p.Z, st);
+  if (rc) return rc;
+  return launch_view_geom(p, p.ps_ang, 1, PN * p.Z, p.ps_vg, p.ps_fc, p.ps_cvd, st);
+}
+
+static int ps_proj_dev(Plan& p, const float* d_angs, int PN, const float* d_vol, float* d_prj, cudaStream_t st) {
+  int rc;
+  if ((rc = ps_alloc(p)) || (rc = ps_geometry(p, d_angs, PN, st))) return rc;
+  const int Z = p.Z;
+  {
+    ProfScope ps(KIND_SAT_IMAGE, st);
+    if ((rc = ps_transpose(d_vol, p.ps_img, 1, (long long)p.XN * p.YN, Z, st)) ||
+        (rc = ps_transpose(p.ps_img, p.ps_imgt, Z, p.YN, p.XN, st)))
+      return rc;
+    PsScanArgs a{};
+    a.mask = p.has_mask ? p.d_mask : nullptr;
+    a.XN = p.XN; a.pad = 1;
+    a.tab = p.ps_tabx; a.nlines = Z * p.YN; a.N = p.XN; a.Nw = p.XN + 2; a.src = p.ps_img; a.lines_per_slice = p.YN;
+    if ((rc = ps_scan(p.mode, 0, a, st))) return rc;
+    a.tab = p.ps_taby; a.nlines = Z * p.XN; a.N = p.YN; a.Nw = p.YN + 2; a.src = p.ps_imgt; a.lines_per_slice = p.XN;
+    a.cols = 1;
+    if ((rc = ps_scan(p.mode, 0, a, st))) return rc;
+  }
+  PsFwdArgs f;
+  f.tabx = p.ps_tabx; f.taby = p.ps_taby; f.vg = p.ps_vg; f.fc = p.ps_fc; f.cvd = p.ps_cvd;
+  f.out = p.ps_sino; f.cstride = PN; f.U = p.U; f.XN = p.XN; f.YN = p.YN; f.dx = (float)p.dx;
+  if ((rc = ps_fwd(p.mode, f, PN, Z, st))) return rc;
+  rc = ps_transpose(p.ps_sino, d_prj, 1, Z, PN * p.U, st);
+  mark_use(p, st);
+  return rc;
+}
+
+static int ps_back_dev(Plan& p, const float* d_angs, int PN, const float* d_prj, float* d_vol, cudaStream_t st) {
+  if (!p.adj_ok) return set_err(DDFAN_ERR_UNSUPPORTED, "detector boundaries are not monotone as seen from the source");
+  int rc;
+  if ((rc = ps_alloc(p)) || (rc = ps_geometry(p, d_angs, PN, st))) return rc;
+  const int Z = p.Z;
+  {
+    // weighted channel prefix sums of every (slice, view) line
+    ProfScope ps(KIND_SAT_SINO, st);
+    if ((rc = ps_transpose(d_prj, p.ps_sino, 1, (long long)PN * p.U, Z, st))) return rc;
+    PsScanArgs a{};
+    a.tab = p.ps_sq; a.nlines = Z * PN; a.N = p.U; a.Nw = p.U + 1; a.src = p.ps_sino; a.lines_per_slice = 1;
+    a.wgt = p.ps_cvd; a.wscale = 1.f;
+    if ((rc = ps_scan(p.mode, 0, a, st))) return rc;
+  }
+  PsBackArgs b{};
+  b.sq = p.ps_sq; b.vg = p.ps_vg; b.fc = p.ps_fc;
+  b.tb = p.d_tb; b.lut = p.d_lut; b.t0 = p.t0; b.invdt = p.invdt; b.dirt = p.dirt; b.M = p.M;
+  b.cnt = PN; b.cstride = PN; b.U = p.U; b.XN = p.XN; b.YN = p.YN;
+  b.ocx = p.ocx; b.ocy = p.ocy; b.dx = p.dx;
+  b.out = p.ps_img; b.mask = p.has_mask ? p.d_mask : nullptr;
+  if ((rc = ps_back(p.mode, b, Z, st))) return rc;
+  rc = ps_transpose(p.ps_img, d_vol, 1, Z, p.XN * p.YN, st);
+  mark_use(p, st);
+  return rc;
+}
+
+int proj_dev_per_slice(Plan& p, const float* d_angs, const float* h_angs, int PN, const float* d_vol,
+                       float* d_prj, cudaStream_t st) {
+  std::vector<std::vector<int>> groups;
+  angle_groups(h_angs, PN, p.Z, groups);
+  if (use_slice_major(p, groups, PN)) return ps_proj_dev(p, d_angs, PN, d_vol, d_prj, st);
+  return for_angle_groups(p, h_angs, PN, [&](const float* da, int zlo, int zhi) {
+    return proj_dev_shared(p, da, 1, PN, d_vol, d_prj, zlo, zhi, st);
+  }, st);
+}
+
+int back_dev_per_slice(Plan& p, const float* d_angs, const float* h_angs, int PN, const float* d_prj,
+                       float* d_vol, int back_mode, cudaStream_t st) {
+  std::vector<std::vector<int>> groups;
+  angle_groups(h_angs, PN, p.Z, groups);
+  if (back_mode == DDFAN_BACK_ADJ && use_slice_major(p, groups, PN))
+    return ps_back_dev(p, d_angs, PN, d_prj, d_vol, st);
+  return for_angle_groups(p, h_angs, PN, [&](const float* da, int zlo, int zhi) {
+    return back_dev_shared(p, da, 1, PN, d_prj, d_vol, back_mode, zlo, zhi, st);
+  }, st);
+}
+
 }  // namespace ddfan
 
 // ====================================================================== C ABI
@@ -775,9 +902,7 @@ DDFAN_API int ddfan_proj_dev(ddfan_plan* plan, const float* d_angs, int PN, int 
   cudaError_t e = cudaMemcpyAsync(h.data(), d_angs, sizeof(float) * h.size(), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "angles download: %s", cudaGetErrorString(e));
-  return for_angle_groups(*p, h.data(), PN, [&](const float* da, int zlo, int zhi) {
-    return proj_dev_shared(*p, da, 1, PN, d_vol, d_prj, zlo, zhi, st);
-  }, st);
+  return proj_dev_per_slice(*p, d_angs, h.data(), PN, d_vol, d_prj, st);
 }
 
 DDFAN_API int ddfan_back_dev(ddfan_plan* plan, const float* d_angs, int PN, int angs_per_slice,
@@ -794,9 +919,7 @@ DDFAN_API int ddfan_back_dev(ddfan_plan* plan, const float* d_angs, int PN, int 
   cudaError_t e = cudaMemcpyAsync(h.data(), d_angs, sizeof(float) * h.size(), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "angles download: %s", cudaGetErrorString(e));
-  return for_angle_groups(*p, h.data(), PN, [&](const float* da, int zlo, int zhi) {
-    return back_dev_shared(*p, da, 1, PN, d_prj, d_vol, back_mode, zlo, zhi, st);
-  }, st);
+  return back_dev_per_slice(*p, d_angs, h.data(), PN, d_prj, d_vol, back_mode, st);
 }
 
 }  // extern "C"

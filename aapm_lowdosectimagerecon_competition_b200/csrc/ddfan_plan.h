@@ -54,6 +54,14 @@ struct Plan {
   float* d_angs = nullptr;  // PNmax angles (host-angle entry points)
   int* d_order = nullptr;   // PNmax views in dispatch order (x-major first)
   int* d_counts = nullptr;  // {x-major views, others}
+  // slice-major buffers for per-slice angle lists (allocated on first use):
+  // geometry rows z * PNmax + m, image [Z][YN][XN] and [Z][XN][YN], sinogram
+  // [Z][PNmax][U], cell tables
+  float* ps_ang = nullptr;
+  ViewGeom* ps_vg = nullptr;
+  double2* ps_fc = nullptr;
+  float *ps_cvd = nullptr, *ps_img = nullptr, *ps_imgt = nullptr, *ps_sino = nullptr;
+  float *ps_tabx = nullptr, *ps_taby = nullptr, *ps_sq = nullptr;
   cudaStream_t alloc_stream = nullptr;  // stream-ordered allocation / release
   cudaEvent_t last_use = nullptr;       // recorded after every call's launches
   size_t bytes = 0;
@@ -73,6 +81,13 @@ void plan_free(Plan* p);
 
 int launch_view_geom(const Plan& p, const float* d_angs, int stride, int PN, ViewGeom* vg,
                      double2* fc, float* cvd, cudaStream_t st);
+// Per-slice angle lists d_angs [PN][Z] (h_angs: the same on the host): one
+// launch group per distinct list, or the slice-major kernels when groups would
+// recompute many slices (exact adjoint and forward only).
+int proj_dev_per_slice(Plan& p, const float* d_angs, const float* h_angs, int PN, const float* d_vol,
+                       float* d_prj, cudaStream_t st);
+int back_dev_per_slice(Plan& p, const float* d_angs, const float* h_angs, int PN, const float* d_prj,
+                       float* d_vol, int back_mode, cudaStream_t st);
 // The prefix-sum builders, the forward projector and the backprojector run
 // only the z-blocks / z-tiles that hold slices [zlo, zhi) (zhi < 0: all);
 // slices outside the range that share a block are computed but not written

@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include "ddfan_device.cuh"
+#include "ddfan_ps.h"
 
 namespace ddfan {
 
@@ -216,34 +217,17 @@ static __global__ void __launch_bounds__(256) k_ps_transpose(const float* __rest
 
 // ---------------------------------------------------------------- prefix sums
 
-// What a slice-major table is built from: lines of an image (one slice's rows
-// or columns) or the OS-SART residual of one (slice, view) of a subset.
-struct PsScanArgs {
-  void* tab;            // cells (PsCell<M>::T), line t at [t * Nw, t * Nw + Nw)
-  int nlines, N, Nw;    // lines, values per line, cells per line (Nw >= N + pad; cells past the values hold the total)
-  int pad;              // zero cells before the values (image tables: 1, the guard cell of clamped samples)
-  // image: src [nlines][N] (slice-major, lines of a slice contiguous); mask [YN][XN]
-  const float* src;
-  const uint8_t* mask;
-  int XN, lines_per_slice, cols;  // cols: line = x column, k = y (mask index k * XN + line)
-  // residual: line = z * cnt + m, table line z * cstride + m; y [Z][P][U]
-  // (views in the caller's order), ax [Z][cstride][U], rows [(roff + m)][U]
-  // (subset order), wgt [Z][cstride][U] or null
-  const float* y;
-  const float* ax;
-  const float* rows;
-  const float* wgt;
-  float wscale;
-  int cnt, cstride, P, roff, ksub, nOS;
-};
-
 template <int KIND>
 __device__ __forceinline__ float ps_value(const PsScanArgs& a, int line, int k) {
   if (k >= a.N) return 0.f;
   if (KIND == 0) {
-    const int l = line % a.lines_per_slice;
-    float v = __ldg(a.src + (size_t)line * a.N + k);
-    if (a.mask) v *= (float)a.mask[a.cols ? (size_t)k * a.XN + l : (size_t)l * a.XN + k];
+    const size_t e = (size_t)line * a.N + k;
+    float v = __ldg(a.src + e);
+    if (a.mask) {
+      const int l = line % a.lines_per_slice;
+      v *= (float)a.mask[a.cols ? (size_t)k * a.XN + l : (size_t)l * a.XN + k];
+    }
+    if (a.wgt) v *= __ldg(a.wgt + e) * a.wscale;
     return v;
   } else {
     // r = (y - A x) / rowSum where rowSum != 0, else A x (AAPM_script/OSSART_AAPM.m:86-88),
@@ -320,17 +304,6 @@ __global__ void __launch_bounds__(128) k_ps_scan(PsScanArgs a) {
 
 // ---------------------------------------------------------------- forward
 
-struct PsFwdArgs {
-  const void* tabx;   // image rows [Z][YN][XN + 2] cells (y-major views), guard cell first and last
-  const void* taby;   // image columns [Z][XN][YN + 2] cells (x-major views)
-  const ViewGeom* vg;   // rows z * cstride + m
-  const double2* fc;    // [rows][U+1] boundary lines
-  const float* cvd;     // [rows][U]
-  float* out;           // [Z][cstride][U]
-  int cstride, U, XN, YN;
-  float dx;
-};
-
 // Branchless DD forward projection (AAPM_script/MultiSlicesProjGPU.cu:100-200)
 // of one slice and one of its views per (blockIdx.z, blockIdx.y).  Lane L of
 // warp w owns boundary b = (tile * 8 + w) * 31 + L; channel b (lanes 0..30)
@@ -385,28 +358,6 @@ __global__ void __launch_bounds__(256) k_ps_fwd(PsFwdArgs a) {
 }
 
 // ---------------------------------------------------------------- exact adjoint
-
-struct PsBackArgs {
-  const void* sq;       // weighted residual table [Z][cstride][U+1] cells
-  const ViewGeom* vg;
-  const double2* fc;
-  const float* tb;      // plan's boundary fan tangents (U+1) and bracket lookup (M)
-  const uint16_t* lut;
-  float t0, invdt, dirt;
-  int M;
-  int cnt, cstride, U, XN, YN;
-  double ocx, ocy, dx;
-  // OS-SART update of x [Z][YN][XN] in place: x += t / colSum where colSum != 0,
-  // else x += t, t the masked backprojection; or, with x null, out = t
-  float* x;
-  const float* colsum;
-  int nonneg;
-  float* out;
-  const uint8_t* mask;
-};
-
-// rows of pixels per warp in k_ps_back_adj (8 warps: 2 across x, 4 down y)
-constexpr int kPsBackRows = 8;
 
 // Exact transpose of k_ps_fwd, both view orientations in one pass.  Warp =
 // 31 consecutive pixels of a row (lanes 0..30) x R rows of one slice; it

@@ -14,7 +14,7 @@
 #include "ddfan.h"
 #include "ddfan_kernels.cuh"
 #include "ddfan_plan.h"
-#include "ddfan_ps_kernels.cuh"
+#include "ddfan_ps.h"
 
 namespace ddfan {
 
@@ -83,7 +83,7 @@ int device_count() {
 }  // namespace
 
 // One slab of a mex-style call on one device: upload, project or backproject
-// (one launch group per distinct angle list), download.
+// (per distinct angle list, or slice-major), download.
 static int mex_slab(bool forward, const PlanDesc& d, const float* angs, int PN, const float* in,
                     float* out, int back_mode) {
   PlanPtr P;
@@ -95,35 +95,15 @@ static int mex_slab(bool forward, const PlanDesc& d, const float* angs, int PN, 
   DevBuf<float> din, dout;
   if ((rc = din.alloc(forward ? V : S)) || (rc = dout.alloc(forward ? S : V))) return rc;
   DDFAN_CK(cudaMemcpy(din.p, in, sizeof(float) * (forward ? V : S), cudaMemcpyHostToDevice));
-  // per-slice angle lists: one launch group per distinct list
-  std::vector<int> rep;
-  std::vector<std::vector<int>> grp;
-  for (int z = 0; z < p.Z; ++z) {
-    int gi = -1;
-    for (size_t k = 0; k < rep.size() && gi < 0; ++k) {
-      bool same = true;
-      for (int q = 0; q < PN && same; ++q)
-        same = std::memcmp(&angs[(size_t)q * p.Z + z], &angs[(size_t)q * p.Z + rep[k]], sizeof(float)) == 0;
-      if (same) gi = (int)k;
-    }
-    if (gi < 0) { rep.push_back(z); grp.push_back({z}); }
-    else grp[gi].push_back(z);
-  }
-  std::vector<float> a(PN);
-  for (auto& gr : grp) {
-    for (int q = 0; q < PN; ++q) a[q] = angs[(size_t)q * p.Z + gr[0]];
-    DDFAN_CK(cudaMemcpy(p.d_angs, a.data(), sizeof(float) * PN, cudaMemcpyHostToDevice));
-    size_t i = 0;
-    while (i < gr.size()) {
-      size_t j = i + 1;
-      while (j < gr.size() && gr[j] == gr[j - 1] + 1) ++j;
-      rc = forward ? proj_dev_shared(p, p.d_angs, 1, PN, din.p, dout.p, gr[i], gr[j - 1] + 1, 0)
-                   : back_dev_shared(p, p.d_angs, 1, PN, din.p, dout.p, back_mode, gr[i], gr[j - 1] + 1, 0);
-      if (rc) return rc;
-      i = j;
-    }
-    DDFAN_CK(cudaDeviceSynchronize());
-  }
+  // per-slice angle lists: one launch group per distinct list, or the
+  // slice-major kernels
+  DevBuf<float> dang;
+  if ((rc = dang.alloc((size_t)PN * p.Z))) return rc;
+  DDFAN_CK(cudaMemcpy(dang.p, angs, sizeof(float) * PN * p.Z, cudaMemcpyHostToDevice));
+  rc = forward ? proj_dev_per_slice(p, dang.p, angs, PN, din.p, dout.p, 0)
+               : back_dev_per_slice(p, dang.p, angs, PN, din.p, dout.p, back_mode, 0);
+  if (rc) return rc;
+  DDFAN_CK(cudaDeviceSynchronize());
   DDFAN_CK(cudaMemcpy(out, dout.p, sizeof(float) * (forward ? S : V), cudaMemcpyDeviceToHost));
   return DDFAN_OK;
 }
@@ -275,49 +255,6 @@ static int gather_slices(const float* src, int Zs, float* dst, int Zd, const int
 
 // ------------------------------------------------------------ slice-major path
 
-static int ps_check(const char* what) {
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "%s launch: %s", what, cudaGetErrorString(e));
-  return DDFAN_OK;
-}
-
-// out[b][c][r] = in[b][r][c]
-static int ps_transpose(const float* in, float* out, int B, long long R, int C, cudaStream_t st) {
-  if (B < 1 || R < 1 || C < 1) return DDFAN_OK;
-  const long long nrt = (R + 31) / 32;
-  dim3 grid((C + 31) / 32, (unsigned)std::min<long long>(nrt, 65535), B);
-  k_ps_transpose<<<grid, 256, 0, st>>>(in, out, R, C);
-  return ps_check("k_ps_transpose");
-}
-
-template <int M, int C, int KIND>
-static void ps_scan_c(const PsScanArgs& a, cudaStream_t st) {
-  constexpr int WPC = C > 24 ? 2 : 4;  // warps (lines) per CTA, as k_ps_scan
-  k_ps_scan<M, C, KIND><<<(a.nlines + WPC - 1) / WPC, 32 * WPC, 0, st>>>(a);
-}
-
-template <int M, int KIND>
-static void ps_scan_go(const PsScanArgs& a, cudaStream_t st) {
-  const int C = (a.N + 31) / 32;
-  if (C <= 8) ps_scan_c<M, 8, KIND>(a, st);
-  else if (C <= 16) ps_scan_c<M, 16, KIND>(a, st);
-  else if (C <= 24) ps_scan_c<M, 24, KIND>(a, st);
-  else ps_scan_c<M, 32, KIND>(a, st);
-}
-
-template <int KIND>
-static int ps_scan(int mode, const PsScanArgs& a, cudaStream_t st) {
-  if (a.N > 1024 || a.Nw < a.N + a.pad)
-    return set_err(DDFAN_ERR_UNSUPPORTED, "slice-major prefix sums: line of %d cells", a.Nw);
-  if (a.nlines < 1) return DDFAN_OK;
-  switch (mode) {
-    case SAT_FP32: ps_scan_go<SAT_FP32, KIND>(a, st); break;
-    case SAT_HILO: ps_scan_go<SAT_HILO, KIND>(a, st); break;
-    default: ps_scan_go<SAT_FP64, KIND>(a, st); break;
-  }
-  return ps_check("k_ps_scan");
-}
-
 // Both image tables of the current image (rows from d_x, columns from its transpose).
 static int ps_sat_image(Solver& s, cudaStream_t st) {
   const Plan& p = *s.P;
@@ -330,30 +267,10 @@ static int ps_sat_image(Solver& s, cudaStream_t st) {
   a.pad = 1;  // guard cells: one before the line, one after (the total)
   a.tab = s.d_tabx; a.nlines = s.Z * s.YN; a.N = s.XN; a.Nw = s.XN + 2; a.src = s.d_x; a.lines_per_slice = s.YN;
   a.cols = 0;
-  if ((rc = ps_scan<0>(p.mode, a, st))) return rc;
+  if ((rc = ps_scan(p.mode, 0, a, st))) return rc;
   a.tab = s.d_taby; a.nlines = s.Z * s.XN; a.N = s.YN; a.Nw = s.YN + 2; a.src = s.d_xt; a.lines_per_slice = s.XN;
   a.cols = 1;
-  return ps_scan<0>(p.mode, a, st);
-}
-
-static int ps_fwd(int mode, const PsFwdArgs& a, int cnt, int Z, cudaStream_t st) {
-  dim3 grid((a.U + 247) / 248, cnt, Z);
-  switch (mode) {
-    case SAT_FP32: k_ps_fwd<SAT_FP32><<<grid, 256, 0, st>>>(a); break;
-    case SAT_HILO: k_ps_fwd<SAT_HILO><<<grid, 256, 0, st>>>(a); break;
-    default: k_ps_fwd<SAT_FP64><<<grid, 256, 0, st>>>(a); break;
-  }
-  return ps_check("k_ps_fwd");
-}
-
-static int ps_back(int mode, const PsBackArgs& a, int Z, cudaStream_t st) {
-  dim3 grid((a.XN + 61) / 62, (a.YN + 4 * kPsBackRows - 1) / (4 * kPsBackRows), Z);
-  switch (mode) {
-    case SAT_FP32: k_ps_back_adj<SAT_FP32><<<grid, 256, 0, st>>>(a); break;
-    case SAT_HILO: k_ps_back_adj<SAT_HILO><<<grid, 256, 0, st>>>(a); break;
-    default: k_ps_back_adj<SAT_FP64><<<grid, 256, 0, st>>>(a); break;
-  }
-  return ps_check("k_ps_back_adj");
+  return ps_scan(p.mode, 0, a, st);
 }
 
 // Subset k of a slice-major iteration: every slice's own views k, k + nOS, ...
@@ -372,7 +289,6 @@ static int ps_subset(Solver& s, int k, cudaStream_t st) {
     if ((rc = ps_sat_image(s, st))) return rc;
   }
   {
-    ProfScope ps(KIND_FWD, st);
     PsFwdArgs f;
     f.tabx = s.d_tabx; f.taby = s.d_taby;
     f.vg = s.d_vg; f.fc = s.d_fc; f.cvd = s.d_cvd; f.out = s.d_ax;
@@ -386,10 +302,9 @@ static int ps_subset(Solver& s, int k, cudaStream_t st) {
     r.tab = s.d_sq; r.nlines = Z * c; r.N = U; r.Nw = U + 1;
     r.y = s.d_y; r.ax = s.d_ax; r.rows = s.d_rows; r.wgt = s.d_cvd; r.wscale = 1.f;
     r.cnt = c; r.cstride = s.cstride; r.P = s.PNall; r.roff = s.off[k]; r.ksub = k; r.nOS = s.nsub;
-    if ((rc = ps_scan<1>(p.mode, r, st))) return rc;
+    if ((rc = ps_scan(p.mode, 1, r, st))) return rc;
   }
   // exact-adjoint backprojection, divide by colSum, add, optional clamp (:91-97)
-  ProfScope ps(KIND_BACK_A, st);
   PsBackArgs b{};
   b.sq = s.d_sq; b.vg = s.d_vg; b.fc = s.d_fc;
   b.tb = p.d_tb; b.lut = p.d_lut; b.t0 = p.t0; b.invdt = p.invdt; b.dirt = p.dirt; b.M = p.M;

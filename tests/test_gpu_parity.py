@@ -58,6 +58,7 @@ CASES = {
     "square": dict(),
     "rect_offcentre_quarter": dict(XN=36, YN=28, cx=3.5, cy=-2.0, dcnt=0.25),
     "masked_perslice": dict(SLN=5, per_slice=True, masked=True),
+    "perslice_rect_odd": dict(SLN=13, XN=36, YN=28, cx=1.5, cy=-2.5, per_slice=True, masked=True),
     "single_slice": dict(SLN=1),
     "odd_slices": dict(SLN=13, XN=24, YN=30),
     "many_slices": dict(SLN=64, XN=32, YN=32, PN=30),
