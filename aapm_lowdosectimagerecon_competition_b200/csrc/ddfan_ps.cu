@@ -85,4 +85,17 @@ int ps_back(int mode, const PsBackArgs& a, int Z, cudaStream_t st) {
   return ps_check("k_ps_back_adj");
 }
 
+int ps_back_ref(int mode, const PsBackArgs& a, int Z, cudaStream_t st) {
+  if (Z < 1) return DDFAN_OK;
+  if (Z > 65535) return set_err(DDFAN_ERR_UNSUPPORTED, "slice-major backprojection: %d slices", Z);
+  dim3 grid((a.XN + 63) / 64, (a.YN + 4 * kPsBackRows - 1) / (4 * kPsBackRows), Z);
+  ProfScope ps(KIND_BACK_A, st);
+  switch (mode) {
+    case SAT_FP32: k_ps_back_ref<SAT_FP32><<<grid, 256, 0, st>>>(a); break;
+    case SAT_HILO: k_ps_back_ref<SAT_HILO><<<grid, 256, 0, st>>>(a); break;
+    default: k_ps_back_ref<SAT_FP64><<<grid, 256, 0, st>>>(a); break;
+  }
+  return ps_check("k_ps_back_ref");
+}
+
 }  // namespace ddfan

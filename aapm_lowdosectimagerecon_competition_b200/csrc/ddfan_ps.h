@@ -53,6 +53,7 @@ struct PsBackArgs {
   int M;
   int cnt, cstride, U, XN, YN;
   double ocx, ocy, dx;
+  double inv_sid, inv_dbeta, cnt_ref;  // REF formula: 1/|source|, 1/(channel angle), detCntIdx + 0.5
   // OS-SART update of x [Z][YN][XN] in place: x += t / colSum where colSum != 0,
   // else x += t, t the masked backprojection; or, with x null, out = t
   float* x;
@@ -72,5 +73,7 @@ int ps_scan(int mode, int kind, const PsScanArgs& a, cudaStream_t st);
 // grid: 31-channel groups x cnt views x Z slices
 int ps_fwd(int mode, const PsFwdArgs& a, int cnt, int Z, cudaStream_t st);
 int ps_back(int mode, const PsBackArgs& a, int Z, cudaStream_t st);
+// the reference backprojector's formula (k_back_ref) in slice-major layout
+int ps_back_ref(int mode, const PsBackArgs& a, int Z, cudaStream_t st);
 
 }  // namespace ddfan

@@ -496,4 +496,71 @@ __global__ void __launch_bounds__(256) k_ps_back_adj(PsBackArgs a) {
   }
 }
 
+// The reference backprojector's formula (AAPM_script/MultiSlicesBackGPU.cu:115-184,
+// as k_back_ref) per slice: voxel-driven, angular detector coordinate
+// alpha = asin(cross / (|s| l)), footprint half-width dx ddv / (2 l^2),
+// weight dx l / ddv, coordinate alpha / dbeta + detCntIdx + 1, all in FP64
+// per (voxel, view), then the two samples of the channel prefix sums in table
+// precision.  Warp = 32 consecutive pixels of a row x R rows of one slice;
+// the OS-SART update (or the plain backprojection) is fused as in
+// k_ps_back_adj, with k_back_ref's mask rule (masked voxels get 0).
+template <int M>
+__global__ void __launch_bounds__(256) k_ps_back_ref(PsBackArgs a) {
+  constexpr int R = kPsBackRows, PX = 32;
+  using Cell = typename PsCell<M>::T;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int z = blockIdx.z;
+  const int x0 = (blockIdx.x * 2 + (w & 1)) * PX, y0 = (blockIdx.y * 4 + (w >> 1)) * R;
+  if (x0 >= a.XN || y0 >= a.YN) return;  // uniform per warp
+  const int ix = x0 + lane;
+  const int U = a.U;
+  const double Ud = (double)U;
+  const size_t rowQ = (size_t)(U + 1);
+  float acc[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) acc[i] = 0.f;
+  for (int m = 0; m < a.cnt; ++m) {
+    const size_t r = (size_t)z * a.cstride + m;
+    const double sx = a.vg[r].sx, sy = a.vg[r].sy;
+    const bool xdom = fabs(sx) > fabs(sy);
+    const Cell* qrow = reinterpret_cast<const Cell*>(a.sq) + r * rowQ;
+    const double ddx = ((double)ix - a.ocx) * a.dx - sx;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const double ddy = ((double)(y0 + i) - a.ocy) * a.dx - sy;
+      const double l2 = ddx * ddx + ddy * ddy;
+      const double ln = sqrt(l2);
+      const double alpha = asin((sy * ddx - sx * ddy) * a.inv_sid / ln);
+      const double ddv = xdom ? ddx : ddy;
+      const double da = ddv / l2 * a.dx * 0.5;
+      const float wt = (float)(a.dx / ddv * ln);
+      const double cL = fmin(fmax((alpha - da) * a.inv_dbeta + a.cnt_ref, 0.0), Ud);
+      const double cR = fmin(fmax((alpha + da) * a.inv_dbeta + a.cnt_ref, 0.0), Ud);
+      const int iL = min((int)cL, U - 1), iR = min((int)cR, U - 1);
+      PhiS<M> pL, pR;
+      pL.load(qrow + iL, (float)(cL - iL));
+      pR.load(qrow + iR, (float)(cR - iR));
+      acc[i] = fmaf(pR.diff(pL), wt, acc[i]);
+    }
+  }
+  if (ix >= a.XN) return;
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int iy = y0 + i;
+    if (iy >= a.YN) break;
+    const size_t pix = (size_t)iy * a.XN + ix;
+    const size_t idx = (size_t)z * a.XN * a.YN + pix;
+    float val = (!a.mask || a.mask[pix] != 0) ? acc[i] : 0.f;
+    if (a.x) {
+      const float cs = __ldg(a.colsum + pix);
+      const float t = cs != 0.f ? __fdiv_rn(val, cs) : val;
+      val = a.x[idx] + t;
+      if (a.nonneg) val = fmaxf(val, 0.f);
+      a.x[idx] = val;
+    } else {
+      a.out[idx] = val;
+    }
+  }
+}
+
 }  // namespace ddfan

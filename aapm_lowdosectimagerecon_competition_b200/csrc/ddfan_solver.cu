@@ -300,19 +300,21 @@ static int ps_subset(Solver& s, int k, cudaStream_t st) {
     ProfScope ps(KIND_SAT_SINO, st);
     PsScanArgs r{};
     r.tab = s.d_sq; r.nlines = Z * c; r.N = U; r.Nw = U + 1;
-    r.y = s.d_y; r.ax = s.d_ax; r.rows = s.d_rows; r.wgt = s.d_cvd; r.wscale = 1.f;
+    r.y = s.d_y; r.ax = s.d_ax; r.rows = s.d_rows; r.wgt = s.back_mode == DDFAN_BACK_ADJ ? s.d_cvd : nullptr;
+    r.wscale = 1.f;
     r.cnt = c; r.cstride = s.cstride; r.P = s.PNall; r.roff = s.off[k]; r.ksub = k; r.nOS = s.nsub;
     if ((rc = ps_scan(p.mode, 1, r, st))) return rc;
   }
-  // exact-adjoint backprojection, divide by colSum, add, optional clamp (:91-97)
+  // backprojection, divide by colSum, add, optional clamp (:91-97)
   PsBackArgs b{};
   b.sq = s.d_sq; b.vg = s.d_vg; b.fc = s.d_fc;
   b.tb = p.d_tb; b.lut = p.d_lut; b.t0 = p.t0; b.invdt = p.invdt; b.dirt = p.dirt; b.M = p.M;
   b.cnt = c; b.cstride = s.cstride; b.U = U; b.XN = s.XN; b.YN = s.YN;
   b.ocx = p.ocx; b.ocy = p.ocy; b.dx = p.dx;
+  b.inv_sid = p.inv_sid; b.inv_dbeta = p.inv_dbeta; b.cnt_ref = (double)p.detCntIdx + 0.5;
   b.x = s.d_x; b.colsum = s.d_cols + (size_t)k * s.XN * s.YN; b.nonneg = s.nonneg;
   b.mask = p.has_mask ? p.d_mask : nullptr;
-  return ps_back(p.mode, b, Z, st);
+  return s.back_mode == DDFAN_BACK_ADJ ? ps_back(p.mode, b, Z, st) : ps_back_ref(p.mode, b, Z, st);
 }
 
 // One OS-SART iteration (AAPM_script/OSSART_AAPM.m:79-115) on stream st.
@@ -537,11 +539,13 @@ static int solver_weights(Solver& s, const PlanDesc& d, const std::vector<float>
 }
 
 // The windowed cost (projector work over that of shared lists) above which
-// the slice-major path is faster.  Measured at 512 x 512 x 128, 24 subsets of
-// 96 views: slice-major iterations take 2.05x the shared-list time whatever
-// the lists; windowed ones 2.13x at a modelled cost of 1.76 (slices 36 raw
-// views apart) and 13.5x at 13.3 (86.07 apart).
-static constexpr double kSliceMajorCost = 1.7;
+// the slice-major path is faster, per backprojector.  Measured at
+// 512 x 512 x 128, 24 subsets of 96 views: slice-major iterations take 2.05x
+// (exact adjoint) and 3.9x (REF, FP64 asin per sample and slice) the
+// shared-list time whatever the lists; windowed ones about 1.2x their
+// modelled cost (2.13x and 2.2x at a model of 1.76 for slices 36 raw views
+// apart, 13.5x at 13.3 for 86.07 apart).
+static constexpr double kSliceMajorCostAdj = 1.7, kSliceMajorCostRef = 3.1;
 
 static int solver_create(Solver** out, float x0, float y0, int DNU, const float* xds, const float* yds,
                          float detCntIdx, float imgXCenter, float imgYCenter, const float* hangs,
@@ -596,14 +600,14 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
     win_cost = best / ((double)PNall * ((SLN + 3) / 4));
   }
   // Per-slice angle lists whose windows share little go to the slice-major
-  // path (exact adjoint only), which costs about kSliceMajorCost times the
-  // shared-list iteration whatever the lists; DDFAN_PER_SLICE=windowed or
-  // =slices overrides the choice (=slices also for shared lists).
+  // path, whose cost relative to shared lists does not depend on the lists; DDFAN_PER_SLICE=windowed or =slices overrides the
+  // choice (=slices also for shared lists).
   {
     const char* pv = getenv("DDFAN_PER_SLICE");
     const bool want_win = pv && !std::strcmp(pv, "windowed");
     const bool want_ps = pv && !std::strcmp(pv, "slices");
-    s.ps = back_mode == DDFAN_BACK_ADJ && (want_ps || (s.win && !want_win && win_cost > kSliceMajorCost));
+    const double threshold = back_mode == DDFAN_BACK_ADJ ? kSliceMajorCostAdj : kSliceMajorCostRef;
+    s.ps = want_ps || (s.win && !want_win && win_cost > threshold);
     if (s.ps) s.win = false;
   }
   if (s.win) {

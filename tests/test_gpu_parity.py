@@ -217,14 +217,14 @@ def rebinned_angles(PN, SLN, starts, BV=0.3):
     return h
 
 
-@pytest.mark.parametrize("back,path", [("ref", "auto"), ("adj", "auto"), ("adj", "windowed")])
+@pytest.mark.parametrize("back,path", [("ref", "auto"), ("ref", "windowed"), ("adj", "auto"), ("adj", "windowed")])
 @pytest.mark.parametrize("lists", ["rebinned", "repeating", "unrelated"])
 def test_ossart_per_slice_angles_matches_oracle(mods, monkeypatch, back, path, lists):
     """OSSART_AAPM with Views(SLN, PN) that differ per slice (the rebinned
     real-data case): every slice is projected with its own angles and the
-    subset weights come from slice 0 (OSSART_AAPM.m:61-64).  The exact
-    adjoint takes the slice-major path by default; the windowed path is
-    checked too."""
+    subset weights come from slice 0 (OSSART_AAPM.m:61-64).  Lists that are
+    not near-identical windows take the slice-major path by default; the
+    windowed path is checked too."""
     dd2, configs, device, O = mods
     if path != "auto":
         monkeypatch.setenv("DDFAN_PER_SLICE", path)
@@ -313,16 +313,18 @@ def per_slice_case(configs, dd2, O, SLN=9, XN=40, YN=36, PN=96, DNU=64, nsub=6, 
 
 @pytest.mark.parametrize("sat,tol", [("fp32", 1e-4), ("hilo", 1e-5), ("fp64", 1e-5)])
 @pytest.mark.parametrize("fista,nonneg", [(1, 0), (0, 1)])
-def test_slice_major_path_matches_oracle(mods, monkeypatch, sat, tol, fista, nonneg):
+@pytest.mark.parametrize("back", ["adj", "ref"])
+def test_slice_major_path_matches_oracle(mods, monkeypatch, sat, tol, fista, nonneg, back):
     """The slice-major path (per-slice geometry, one slice per lane group) in
-    every cell format, on a rectangular image with irregular per-slice lists."""
+    every cell format and with both backprojectors, on a rectangular image
+    with irregular per-slice lists."""
     dd2, configs, device, O = mods
     monkeypatch.setenv("DDFAN_PER_SLICE", "slices")
     s, (x0, y0, xds, yds), h, mask, y = per_slice_case(configs, dd2, O)
     init = np.zeros((s.YN, s.XN, s.SLN), np.float32)
-    xg = dd2.OSSART_AAPM(y, h, init, s.conf(), 3, s.numOfOS, mask, fista, nonneg, sat=sat, back="adj")
+    xg = dd2.OSSART_AAPM(y, h, init, s.conf(), 3, s.numOfOS, mask, fista, nonneg, sat=sat, back=back)
     xo = O.ossart(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0, 0, h, s.PN, s.XN, s.YN, s.SLN, y, init, s.dx, mask, 3,
-                  s.numOfOS, fista, nonneg, O.ADJ)
+                  s.numOfOS, fista, nonneg, O.ADJ if back == "adj" else O.REF)
     assert rel(xg, xo) < tol
     if nonneg and not fista:
         assert xg.min() >= 0
