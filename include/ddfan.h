@@ -127,8 +127,10 @@ DDFAN_API int ddfan_release_cached(int device);
 
 /* Forward projection of device vol[YN][XN][SLN] into device prj[PN][DNU][SLN].
  * d_angs: device view angles; angs_per_slice = 0: d_angs[PN] shared by all
- * slices; 1: d_angs[PN][SLN] (the reference's hangs layout; slices whose
- * angle lists differ are projected one group at a time).  Asynchronous on
+ * slices; 1: d_angs[PN][SLN] (the reference's hangs layout; slices with the
+ * same list are projected together, and when many lists differ -- rebinned
+ * data -- every slice runs with its own geometry on slice-major kernels,
+ * whose buffers the plan allocates on the first such call).  Asynchronous on
  * `stream` (a cudaStream_t, NULL = legacy default stream). */
 DDFAN_API int ddfan_proj_dev(ddfan_plan* plan, const float* d_angs, int PN, int angs_per_slice,
                              const float* d_vol, float* d_prj, void* stream);
