@@ -258,7 +258,6 @@ static int gather_slices(const float* src, int Zs, float* dst, int Zd, const int
 // Both image tables of the current image (rows from d_x, columns from its transpose).
 static int ps_sat_image(Solver& s, cudaStream_t st) {
   const Plan& p = *s.P;
-  const size_t V = (size_t)s.XN * s.YN * s.Z;
   int rc;
   if ((rc = ps_transpose(s.d_x, s.d_xt, s.Z, s.YN, s.XN, st))) return rc;
   PsScanArgs a{};
@@ -277,7 +276,6 @@ static int ps_sat_image(Solver& s, cudaStream_t st) {
 static int ps_subset(Solver& s, int k, cudaStream_t st) {
   const Plan& p = *s.P;
   const int Z = s.Z, U = s.U, c = s.cnt[k];
-  const size_t V = (size_t)s.XN * s.YN * Z;
   const size_t rows = (size_t)Z * s.cstride;
   int rc;
   // geometry of every slice's views of the subset
