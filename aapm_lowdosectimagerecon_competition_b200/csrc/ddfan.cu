@@ -700,12 +700,23 @@ static int ps_alloc(Plan& p) {
   size_t& B = p.bytes;
   cudaStream_t as = p.alloc_stream;
   int rc;
+  const size_t B0 = B;
   if ((rc = dalloc(&p.ps_ang, R, &B, as)) || (rc = dalloc(&p.ps_vg, R, &B, as)) ||
       (rc = dalloc(&p.ps_fc, R * (U + 1), &B, as)) || (rc = dalloc(&p.ps_cvd, R * U, &B, as)) ||
       (rc = dalloc(&p.ps_img, V, &B, as)) || (rc = dalloc(&p.ps_imgt, V, &B, as)) ||
       (rc = dalloc(&p.ps_sino, R * U, &B, as)) || (rc = dalloc(&p.ps_tabx, CF * VG, &B, as)) ||
-      (rc = dalloc(&p.ps_taby, CF * VG, &B, as)) || (rc = dalloc(&p.ps_sq, CF * R * (U + 1), &B, as)))
+      (rc = dalloc(&p.ps_taby, CF * VG, &B, as)) || (rc = dalloc(&p.ps_sq, CF * R * (U + 1), &B, as))) {
+    // release what was taken, so that a later call starts from nothing
+    void** bufs[] = {(void**)&p.ps_ang, (void**)&p.ps_vg, (void**)&p.ps_fc, (void**)&p.ps_cvd,
+                     (void**)&p.ps_img, (void**)&p.ps_imgt, (void**)&p.ps_sino, (void**)&p.ps_tabx,
+                     (void**)&p.ps_taby, (void**)&p.ps_sq};
+    for (void** q : bufs) {
+      dev_free(*q, as);
+      *q = nullptr;
+    }
+    B = B0;
     return rc;
+  }
   // the allocations complete before any stream uses them
   cudaError_t e = cudaStreamSynchronize(as);
   if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "slice-major buffers: %s", cudaGetErrorString(e));
