@@ -59,7 +59,12 @@ DDFAN_API int ddfan_version(void);
 DDFAN_API int ddfan_tune_set_zl(int zblocks, int zl);
 DDFAN_API int ddfan_tune_get_zl(int zblocks);
 /* device bytes ddfan_plan_create / ddfan_ossart_create would allocate
- * (the solver figure includes its transient set-up buffers); 0 = bad sizes */
+ * (the solver figure includes its transient set-up buffers); 0 = bad sizes.
+ * Both are for one angle list shared by all slices.  Per-slice lists take
+ * more: a solver on the slice-major path about 16 B x (XN+2) x (YN+2) x SLN
+ * x 2 for its tables plus 2 x 4 B x PNall x DNU x SLN for the sinogram and
+ * its staging, and a plan's first per-slice call on the slice-major kernels
+ * about 20 B x (DNU+1) x PN x SLN plus the same image tables. */
 DDFAN_API size_t ddfan_plan_estimate_bytes(int XN, int YN, int DNU, int SLN, int PNmax, int sat_mode);
 DDFAN_API size_t ddfan_ossart_estimate_bytes(int XN, int YN, int DNU, int SLN, int PNall, int numOfOS,
                                              int sat_mode);
