@@ -64,7 +64,7 @@ DDFAN_API int ddfan_tune_get_zl(int zblocks);
  * more: a solver on the slice-major path about 16 B x (XN+2) x (YN+2) x SLN
  * x 2 for its tables plus 2 x 4 B x PNall x DNU x SLN for the sinogram and
  * its staging, and a plan's first per-slice call on the slice-major kernels
- * about 20 B x (DNU+1) x PN x SLN plus the same image tables. */
+ * about 40 B x (DNU+1) x PNmax x SLN plus the same image tables. */
 DDFAN_API size_t ddfan_plan_estimate_bytes(int XN, int YN, int DNU, int SLN, int PNmax, int sat_mode);
 DDFAN_API size_t ddfan_ossart_estimate_bytes(int XN, int YN, int DNU, int SLN, int PNall, int numOfOS,
                                              int sat_mode);
