@@ -369,3 +369,19 @@ def test_slice_major_device_api_and_graphs(mods, monkeypatch):
         res.append(sv.image().cpu().numpy())
         sv.close()
     np.testing.assert_array_equal(res[0], res[1])
+
+
+@pytest.mark.parametrize("back", ["adj", "ref"])
+def test_slice_major_uneven_subsets_and_odd_channels(mods, monkeypatch, back):
+    """The slice-major solver when the views do not split evenly (98 views in
+    5 subsets: 20, 20, 20, 19, 19 -- rows past a short subset's count are
+    never read) and the channels do not fill the 31-channel warp groups (61)."""
+    dd2, configs, device, O = mods
+    monkeypatch.setenv("DDFAN_PER_SLICE", "slices")
+    s, (x0, y0, xds, yds), h, mask, y = per_slice_case(configs, dd2, O, SLN=6, XN=34, YN=34, PN=98, DNU=61,
+                                                       nsub=5, seed=8)
+    init = np.zeros((s.YN, s.XN, s.SLN), np.float32)
+    xg = dd2.OSSART_AAPM(y, h, init, s.conf(), 3, s.numOfOS, mask, 1, 0, sat="hilo", back=back)
+    xo = O.ossart(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0, 0, h, s.PN, s.XN, s.YN, s.SLN, y, init, s.dx, mask, 3,
+                  s.numOfOS, 1, 0, O.ADJ if back == "adj" else O.REF)
+    assert rel(xg, xo) < 1e-5
