@@ -498,9 +498,10 @@ __global__ void __launch_bounds__(256) k_ps_back_adj(PsBackArgs a) {
 
 // The reference backprojector's formula (AAPM_script/MultiSlicesBackGPU.cu:115-184,
 // as k_back_ref) per slice: voxel-driven, angular detector coordinate
-// alpha = asin(cross / (|s| l)), footprint half-width dx ddv / (2 l^2),
-// weight dx l / ddv, coordinate alpha / dbeta + detCntIdx + 1, all in FP64
-// per (voxel, view), then the two samples of the channel prefix sums in table
+// alpha = asin(cross / (|s| l)) (here as the equal atan(cross / dot), in
+// FP64), footprint half-width dx ddv / (2 l^2) and weight dx l / ddv (FP32,
+// relative terms), coordinate alpha / dbeta + detCntIdx + 1 in FP64 per
+// (voxel, view), then the two samples of the channel prefix sums in table
 // precision.  Warp = 32 consecutive pixels of a row x R rows of one slice;
 // the OS-SART update (or the plain backprojection) is fused as in
 // k_ps_back_adj, with k_back_ref's mask rule (masked voxels get 0).
@@ -516,6 +517,7 @@ __global__ void __launch_bounds__(256) k_ps_back_ref(PsBackArgs a) {
   const int U = a.U;
   const double Ud = (double)U;
   const size_t rowQ = (size_t)(U + 1);
+  const float dxf = (float)a.dx, hdx = (float)(a.dx * 0.5);
   float acc[R];
 #pragma unroll
   for (int i = 0; i < R; ++i) acc[i] = 0.f;
@@ -528,12 +530,15 @@ __global__ void __launch_bounds__(256) k_ps_back_ref(PsBackArgs a) {
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       const double ddy = ((double)(y0 + i) - a.ocy) * a.dx - sy;
-      const double l2 = ddx * ddx + ddy * ddy;
-      const double ln = sqrt(l2);
-      const double alpha = asin((sy * ddx - sx * ddy) * a.inv_sid / ln);
-      const double ddv = xdom ? ddx : ddy;
-      const double da = ddv / l2 * a.dx * 0.5;
-      const float wt = (float)(a.dx / ddv * ln);
+      // alpha = asin((s_y d_x - s_x d_y) / (|s| l)) is the signed angle between
+      // -s and d: atan of the cross over the dot product (dot > 0 for voxels in
+      // front of the source), which needs no square root in FP64; the
+      // half-width and the weight only need FP32
+      const double alpha = atan((sy * ddx - sx * ddy) / -(sx * ddx + sy * ddy));
+      const float fx = (float)ddx, fy = (float)ddy, fdv = xdom ? fx : fy;
+      const float l2 = fmaf(fx, fx, fy * fy);
+      const double da = (double)(__fdividef(fdv, l2) * hdx);
+      const float wt = __fdividef(dxf, fdv) * sqrtf(l2);
       const double cL = fmin(fmax((alpha - da) * a.inv_dbeta + a.cnt_ref, 0.0), Ud);
       const double cR = fmin(fmax((alpha + da) * a.inv_dbeta + a.cnt_ref, 0.0), Ud);
       const int iL = min((int)cL, U - 1), iR = min((int)cR, U - 1);
