@@ -385,3 +385,28 @@ def test_slice_major_uneven_subsets_and_odd_channels(mods, monkeypatch, back):
     xo = O.ossart(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0, 0, h, s.PN, s.XN, s.YN, s.SLN, y, init, s.dx, mask, 3,
                   s.numOfOS, 1, 0, O.ADJ if back == "adj" else O.REF)
     assert rel(xg, xo) < 1e-5
+
+
+@pytest.mark.parametrize("lists", ["shared", "per_slice"])
+def test_slab_sharded_solve_matches_full(mods, monkeypatch, lists):
+    """One reconstruction split into the slabs of two ranks (solved one after
+    the other here, on one GPU) equals the whole solve: slices are independent
+    and, with per-slice lists, each slab solves global slice 0 first for the
+    subset weights."""
+    from aapm_lowdosectimagerecon_competition_b200 import shard
+    dd2, configs, device, O = mods
+    if lists == "shared":
+        s, (x0, y0, xds, yds), xt, mask, y = solver_case(configs, dd2, O, SLN=9)
+        h = s.hangs()
+    else:
+        monkeypatch.setenv("DDFAN_PER_SLICE", "slices")
+        s, (x0, y0, xds, yds), h, mask, y = per_slice_case(configs, dd2, O, SLN=9)
+    init = np.zeros((s.YN, s.XN, s.SLN), np.float32)
+    kw = dict(mask=mask, numOfOS=s.numOfOS, useFISTA=1, nonneg=1, sat="hilo", back="adj")
+    _, _, whole = shard.solve_slab(x0, y0, s.DNU, xds, yds, s.detCntIdx, h, s.XN, s.YN, s.dx, y, init, 3, 0, 1,
+                                   **kw)
+    parts = [shard.solve_slab(x0, y0, s.DNU, xds, yds, s.detCntIdx, h, s.XN, s.YN, s.dx, y, init, 3, r, 2, **kw)
+             for r in range(2)]
+    assert [(a, b) for a, b, _ in parts] == [(0, 5), (5, 9)]
+    joined = np.concatenate([img.cpu().numpy() for _, _, img in parts], axis=-1)
+    assert rel(joined, whole.cpu().numpy()) < 1e-6

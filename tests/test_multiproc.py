@@ -69,3 +69,40 @@ def test_admission_policy():
     assert serve.pick_admission([5 * gb, 2 * gb], used=0, budget=4 * gb, backfill=1) is None
     assert serve.pick_admission([], used=0, budget=4 * gb, backfill=4) is None
     assert serve.pick_admission([3 * gb], used=2 * gb, budget=4 * gb, backfill=4) is None
+
+
+def _gather_worker(rank, world, port, q):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    SLN = 7
+    a, b = shard.slice_slab(SLN, rank, world)
+    # slab of a (YN=2, XN=3) image whose slice z holds z + 0.5
+    slab = (torch.arange(a, b, dtype=torch.float32) + 0.5).expand(2, 3, b - a).contiguous()
+    full = shard.gather_slabs(slab, SLN, rank, world)
+    q.put((rank, full.tolist()))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_ranks_gather_uneven_slabs():
+    """A sharded image comes back whole on every rank (slabs of 4 and 3 of 7
+    slices, padded for the all_gather and trimmed)."""
+    import torch
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_gather_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    expect = (torch.arange(7, dtype=torch.float32) + 0.5).expand(2, 3, 7).tolist()
+    for _, full in res:
+        assert full == expect
