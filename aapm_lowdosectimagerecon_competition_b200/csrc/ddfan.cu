@@ -685,7 +685,7 @@ static long long grouped_slices(const Plan& p, const std::vector<std::vector<int
 
 // Time per slice of the slice-major kernels over the shared-list ones,
 // measured at 512 x 512, 96 views: forward 1.45x, exact adjoint 2.7x, REF
-// backprojector 5.5x (its FP64 geometry per sample is no longer shared by 32
+// backprojector 4.4x (its FP64 geometry per sample is no longer shared by 32
 // slices).  The grouped path costs its computed slices over Z times the
 // shared-list time.
 static bool use_slice_major(const Plan& p, const std::vector<std::vector<int>>& groups, int PN, double ratio) {
@@ -800,7 +800,7 @@ int back_dev_per_slice(Plan& p, const float* d_angs, const float* h_angs, int PN
                        float* d_vol, int back_mode, cudaStream_t st) {
   std::vector<std::vector<int>> groups;
   angle_groups(h_angs, PN, p.Z, groups);
-  if (use_slice_major(p, groups, PN, back_mode == DDFAN_BACK_ADJ ? 2.7 : 5.5))
+  if (use_slice_major(p, groups, PN, back_mode == DDFAN_BACK_ADJ ? 2.7 : 4.4))
     return ps_back_dev(p, d_angs, PN, d_prj, d_vol, back_mode, st);
   return for_angle_groups(p, h_angs, PN, [&](const float* da, int zlo, int zhi) {
     return back_dev_shared(p, da, 1, PN, d_prj, d_vol, back_mode, zlo, zhi, st);

@@ -527,14 +527,30 @@ __global__ void __launch_bounds__(256) k_ps_back_ref(PsBackArgs a) {
     const bool xdom = fabs(sx) > fabs(sy);
     const Cell* qrow = reinterpret_cast<const Cell*>(a.sq) + r * rowQ;
     const double ddx = ((double)ix - a.ocx) * a.dx - sx;
+    double alpha = 0.0, ddy_prev = 0.0;
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       const double ddy = ((double)(y0 + i) - a.ocy) * a.dx - sy;
-      // alpha = asin((s_y d_x - s_x d_y) / (|s| l)) is the signed angle between
-      // -s and d: atan of the cross over the dot product (dot > 0 for voxels in
-      // front of the source), which needs no square root in FP64; the
-      // half-width and the weight only need FP32
-      const double alpha = atan((sy * ddx - sx * ddy) / -(sx * ddx + sy * ddy));
+      // alpha = asin((s_y d_x - s_x d_y) / (|s| l)) is the signed angle from
+      // -s to d: atan of the cross over the dot product (dot > 0 for voxels in
+      // front of the source), which needs no square root in FP64.  Down the
+      // column the angle moves by the angle from the previous row's d to this
+      // one, whose tangent t = d_x (dy_i - dy_{i-1}) / (d_{i-1} . d_i) is exact
+      // and small; for |t| <= 0.05 the series t - t^3/3 + t^5/5 - t^7/7 is
+      // exact to FP64 rounding (next term below 2e-13 t), otherwise the full
+      // atan.  The half-width and the weight only need FP32.
+      bool full = i == 0;
+      if (!full) {
+        const double t = ddx * (ddy - ddy_prev) / fma(ddy_prev, ddy, ddx * ddx);
+        if (fabs(t) <= 0.05) {
+          const double t2 = t * t;
+          alpha += t * fma(t2, fma(t2, fma(t2, -1.0 / 7.0, 1.0 / 5.0), -1.0 / 3.0), 1.0);
+        } else {
+          full = true;
+        }
+      }
+      if (full) alpha = atan((sy * ddx - sx * ddy) / -(sx * ddx + sy * ddy));
+      ddy_prev = ddy;
       const float fx = (float)ddx, fy = (float)ddy, fdv = xdom ? fx : fy;
       const float l2 = fmaf(fx, fx, fy * fy);
       const double da = (double)(__fdividef(fdv, l2) * hdx);

@@ -539,11 +539,11 @@ static int solver_weights(Solver& s, const PlanDesc& d, const std::vector<float>
 // The windowed cost (projector work over that of shared lists) above which
 // the slice-major path is faster, per backprojector.  Measured at
 // 512 x 512 x 128, 24 subsets of 96 views: slice-major iterations take 2.05x
-// (exact adjoint) and 3.5x (REF, FP64 atan per sample and slice) the
+// (exact adjoint) and 2.9x (REF, FP64 geometry per sample and slice) the
 // shared-list time whatever the lists; windowed ones about 1.2x their
 // modelled cost (2.13x and 2.2x at a model of 1.76 for slices 36 raw views
 // apart, 13.5x at 13.3 for 86.07 apart).
-static constexpr double kSliceMajorCostAdj = 1.7, kSliceMajorCostRef = 2.9;
+static constexpr double kSliceMajorCostAdj = 1.7, kSliceMajorCostRef = 2.4;
 
 static int solver_create(Solver** out, float x0, float y0, int DNU, const float* xds, const float* yds,
                          float detCntIdx, float imgXCenter, float imgYCenter, const float* hangs,
