@@ -485,13 +485,16 @@ static void win_layout(const std::vector<int>& off, int NG, int T, int nOS, int 
 }
 
 // Row sums and column sums of every subset from slice 0's angles, on a
-// one-slice plan (AAPM_script/OSSART_AAPM.m:57-66).  The row sums of all views
-// go in one forward launch (views are independent; one subset's launch fills
-// a small part of the GPU).  The column sums stay one subset at a time on the
-// solver's stream: spreading them over side streams cut a lone solver's
-// set-up by 5 ms but cost batched solves 20 % of their throughput, as those
-// latency-bound one-slice launches took SM slots from the other solves.
-static int solver_weights(Solver& s, const PlanDesc& d, const std::vector<float>& angs0, int PNmax, cudaStream_t st) {
+// one-slice plan (AAPM_script/OSSART_AAPM.m:57-66), with the 4-slice cell
+// kernels: the REF backprojector's weights, and the exact adjoint's for more
+// than 65535 geometry rows.
+// The row sums of all views go in one forward launch; the column sums one
+// subset at a time on the solver's stream (spreading them over side streams
+// cut a lone solver's set-up by 5 ms but cost batched solves 20 % of their
+// throughput, as those latency-bound one-slice launches took SM slots from
+// the other solves).
+static int solver_weights_cells(Solver& s, const PlanDesc& d, const std::vector<float>& angs0, int PNmax,
+                                cudaStream_t st) {
   const int XN = s.XN, YN = s.YN, DNU = s.U, P = s.PNall;
   PlanDesc d1 = d;
   d1.SLN = 1;
@@ -532,6 +535,86 @@ static int solver_weights(Solver& s, const PlanDesc& d, const std::vector<float>
                           counts.p + 2 * k, c, e, st)))
       return rc;
   }
+  DDFAN_CK(cudaStreamSynchronize(st));
+  return DDFAN_OK;
+}
+
+// Row sums and column sums of every subset from slice 0's angles
+// (AAPM_script/OSSART_AAPM.m:57-66) on the slice-major kernels, which carry
+// one slice without the 4-slice cells' padding: the row sums of all views in
+// one forward launch, and the column sums of all subsets in one
+// backprojection launch, subset k standing in the place of slice k (its views
+// are rows k * cs + m; the pad rows of a short subset backproject zeros).
+// The exact adjoint only: the slice-major REF backprojector takes its
+// half-width and weight in FP32, and column sums divide every update, so the
+// REF weights stay on the cell kernels' FP64 formula.
+static int solver_weights(Solver& s, const PlanDesc& d, const std::vector<float>& angs0, int PNmax,
+                          cudaStream_t st) {
+  const int XN = s.XN, YN = s.YN, DNU = s.U, nsub = s.nsub, cs = PNmax;
+  const size_t R = (size_t)nsub * cs;  // geometry rows [nsub][cs]
+  const bool adj = s.back_mode == DDFAN_BACK_ADJ;
+  if (R > 65535 || !adj) return solver_weights_cells(s, d, angs0, PNmax, st);
+  PlanDesc d1 = d;
+  d1.SLN = 1;
+  d1.PNmax = 1;
+  d1.zl_force = 0;
+  PlanPtr P1;
+  int rc = plan_create(&P1.p, d1);
+  if (rc) return rc;
+  const Plan& p = *P1.p;
+  if (!p.adj_ok) return set_err(DDFAN_ERR_UNSUPPORTED, "detector boundaries are not monotone as seen from the source");
+  // angles [nsub][cs] and the ones to project: an image of ones and, per
+  // subset, cs rows of ones over its views (zeros on pad rows)
+  std::vector<float> wa(R, 0.f), himg((size_t)XN * YN, 1.f), hsino(R * DNU, 0.f);
+  DevBuf<float> ang(st), img(st), ones(st), rows(st), sino(st);
+  DevBuf<ViewGeom> vg(st);
+  DevBuf<double2> fc(st);
+  DevBuf<float> cvd(st);
+  const size_t CF = p.mode == SAT_FP32 ? 2 : 4;  // floats per slice-major cell
+  DevBuf<float> tabx(st), taby(st), sq(st);
+  if ((rc = ang.alloc(R)) || (rc = vg.alloc(R)) || (rc = fc.alloc(R * (DNU + 1))) || (rc = cvd.alloc(R * DNU)) ||
+      (rc = img.alloc((size_t)XN * YN)) || (rc = rows.alloc(R * DNU)) || (rc = sino.alloc(R * DNU)) ||
+      (rc = tabx.alloc(CF * (XN + 2) * YN)) || (rc = taby.alloc(CF * (YN + 2) * XN)) ||
+      (rc = sq.alloc(CF * R * (DNU + 1))))
+    return rc;
+  for (int k = 0; k < nsub; ++k)
+    for (int m = 0; m < s.cnt[k]; ++m) wa[(size_t)k * cs + m] = angs0[(size_t)s.off[k] + m];
+  DDFAN_CK(cudaMemcpyAsync(ang.p, wa.data(), sizeof(float) * R, cudaMemcpyHostToDevice, st));
+  for (int k = 0; k < nsub; ++k)
+    std::fill(hsino.begin() + (size_t)k * cs * DNU, hsino.begin() + ((size_t)k * cs + s.cnt[k]) * DNU, 1.f);
+  DDFAN_CK(cudaMemcpyAsync(img.p, himg.data(), sizeof(float) * XN * YN, cudaMemcpyHostToDevice, st));
+  DDFAN_CK(cudaMemcpyAsync(sino.p, hsino.data(), sizeof(float) * R * DNU, cudaMemcpyHostToDevice, st));
+  if ((rc = launch_view_geom(p, ang.p, 1, (int)R, vg.p, fc.p, cvd.p, st))) return rc;
+  // prefix-sum tables of the masked ones image (rows and columns: the image is its own transpose)
+  PsScanArgs a{};
+  a.mask = p.has_mask ? p.d_mask : nullptr;
+  a.XN = XN; a.pad = 1; a.src = img.p;
+  a.tab = tabx.p; a.nlines = YN; a.N = XN; a.Nw = XN + 2; a.lines_per_slice = YN;
+  if ((rc = ps_scan(p.mode, 0, a, st))) return rc;
+  a.tab = taby.p; a.nlines = XN; a.N = YN; a.Nw = YN + 2; a.lines_per_slice = XN; a.cols = 1;
+  if ((rc = ps_scan(p.mode, 0, a, st))) return rc;
+  // row sums: every view row of the one slice, then into subset order
+  PsFwdArgs f;
+  f.tabx = tabx.p; f.taby = taby.p; f.vg = vg.p; f.fc = fc.p; f.cvd = cvd.p;
+  f.out = rows.p; f.cstride = (int)R; f.U = DNU; f.XN = XN; f.YN = YN; f.dx = (float)p.dx;
+  if ((rc = ps_fwd(p.mode, f, (int)R, 1, st))) return rc;
+  for (int k = 0; k < nsub; ++k)
+    DDFAN_CK(cudaMemcpyAsync(s.d_rows + (size_t)s.off[k] * DNU, rows.p + (size_t)k * cs * DNU,
+                             sizeof(float) * s.cnt[k] * DNU, cudaMemcpyDeviceToDevice, st));
+  // column sums: subset k as slice k, weighted like the solver's residual
+  PsScanArgs q{};
+  q.tab = sq.p; q.nlines = (int)R; q.N = DNU; q.Nw = DNU + 1; q.src = sino.p; q.lines_per_slice = 1;
+  q.wgt = cvd.p; q.wscale = 1.f;
+  if ((rc = ps_scan(p.mode, 0, q, st))) return rc;
+  PsBackArgs b{};
+  b.sq = sq.p; b.vg = vg.p; b.fc = fc.p;
+  b.tb = p.d_tb; b.lut = p.d_lut; b.t0 = p.t0; b.invdt = p.invdt; b.dirt = p.dirt; b.M = p.M;
+  b.cnt = cs; b.cstride = cs; b.U = DNU; b.XN = XN; b.YN = YN;
+  b.ocx = p.ocx; b.ocy = p.ocy; b.dx = p.dx;
+  b.inv_sid = p.inv_sid; b.inv_dbeta = p.inv_dbeta; b.cnt_ref = (double)p.detCntIdx + 0.5;
+  b.out = s.d_cols; b.mask = p.has_mask ? p.d_mask : nullptr;
+  if ((rc = ps_back(p.mode, b, nsub, st))) return rc;
+  // the pageable host sources above are consumed and the temporaries free after this
   DDFAN_CK(cudaStreamSynchronize(st));
   return DDFAN_OK;
 }
@@ -757,10 +840,13 @@ DDFAN_API size_t ddfan_ossart_estimate_bytes(int XN, int YN, int DNU, int SLN, i
                      3 * P * sizeof(int) + 2 * (size_t)numOfOS * sizeof(int) + P * U * sizeof(float) +
                      (size_t)numOfOS * XN * YN * sizeof(float) + P * U * SLN * sizeof(float) +
                      2 * V * sizeof(float) + PNmax * U * SLN * sizeof(float) + sizeof(double);
-  // transient at creation: the one-slice weight plan and its buffers
-  const size_t weights = ddfan_plan_estimate_bytes(XN, YN, DNU, 1, (int)PNmax, sat_mode) +
-                         P * sizeof(ViewGeom) + P * (U + 1) * sizeof(double2) +
-                         (std::max((size_t)XN * YN, PNmax * U) + P * U + 3 * P + 2 * (size_t)numOfOS + 2) * sizeof(float);
+  // transient at creation: the one-slice weight plan and the slice-major
+  // weight buffers (geometry, row sums, ones, tables) over nsub x PNmax rows
+  const size_t R = (size_t)numOfOS * PNmax, CB = sat_mode == SAT_FP32 ? 8 : 16;
+  const size_t weights = ddfan_plan_estimate_bytes(XN, YN, DNU, 1, 1, sat_mode) +
+                         R * (sizeof(ViewGeom) + (U + 1) * sizeof(double2) + sizeof(float) + 3 * U * sizeof(float) +
+                              (U + 1) * CB) +
+                         (size_t)XN * YN * sizeof(float) + ((size_t)(XN + 2) * YN + (size_t)(YN + 2) * XN) * CB;
   return plan + own + weights;
 }
 
