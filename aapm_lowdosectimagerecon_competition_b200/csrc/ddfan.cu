@@ -771,7 +771,7 @@ static int ps_back_dev(Plan& p, const float* d_angs, int PN, const float* d_prj,
     PsScanArgs a{};
     a.tab = p.ps_sq; a.nlines = Z * PN; a.N = p.U; a.Nw = p.U + 1; a.src = p.ps_sino; a.lines_per_slice = 1;
     a.wgt = adj ? p.ps_cvd : nullptr; a.wscale = 1.f;
-    if ((rc = ps_scan(p.mode, 0, a, st))) return rc;
+    if ((rc = ps_scan(p.mode, adj ? 2 : 0, a, st))) return rc;
   }
   PsBackArgs b{};
   b.sq = p.ps_sq; b.vg = p.ps_vg; b.fc = p.ps_fc;

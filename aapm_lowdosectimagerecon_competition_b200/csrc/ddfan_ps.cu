@@ -54,7 +54,8 @@ int ps_scan(int mode, int kind, const PsScanArgs& a, cudaStream_t st) {
     return set_err(DDFAN_ERR_UNSUPPORTED, "slice-major prefix sums: %d values in %d cells", a.N, a.Nw);
   if (a.nlines < 1) return DDFAN_OK;
   if (kind == 0) ps_scan_kind<0>(mode, a, st);
-  else ps_scan_kind<1>(mode, a, st);
+  else if (kind == 1) ps_scan_kind<1>(mode, a, st);
+  else ps_scan_kind<2>(mode, a, st);
   return ps_check("k_ps_scan");
 }
 

@@ -17,7 +17,7 @@ struct PsScanArgs {
   int nlines, N, Nw;    // lines, values per line, cells per line (Nw >= N + pad; cells past the values hold the total)
   int pad;              // zero cells before the values (image tables: 1, the guard cell of clamped samples)
   // kind 0: src [nlines][N] (slice-major, lines of a slice contiguous), times the
-  // image mask [YN][XN] if given and the weight wgt [nlines][N] * wscale if given
+  // image mask [YN][XN] if given; kind 2: src times the weight wgt [nlines][N] * wscale
   const float* src;
   const uint8_t* mask;
   int XN, lines_per_slice, cols;  // cols: line = x column, k = y (mask index k * XN + line)
@@ -68,7 +68,7 @@ constexpr int kPsBackRows = 8;
 
 // out[b][c][r] = in[b][r][c] for b < B, r < R, c < C
 int ps_transpose(const float* in, float* out, int B, long long R, int C, cudaStream_t st);
-// kind 0: image or plain weighted lines; kind 1: OS-SART residual lines
+// kind 0: image lines (masked); kind 1: OS-SART residual lines; kind 2: weighted lines
 int ps_scan(int mode, int kind, const PsScanArgs& a, cudaStream_t st);
 // grid: 31-channel groups x cnt views x Z slices
 int ps_fwd(int mode, const PsFwdArgs& a, int cnt, int Z, cudaStream_t st);

@@ -227,8 +227,10 @@ __device__ __forceinline__ float ps_value(const PsScanArgs& a, int line, int k) 
       const int l = line % a.lines_per_slice;
       v *= (float)a.mask[a.cols ? (size_t)k * a.XN + l : (size_t)l * a.XN + k];
     }
-    if (a.wgt) v *= __ldg(a.wgt + e) * a.wscale;
     return v;
+  } else if (KIND == 2) {
+    const size_t e = (size_t)line * a.N + k;
+    return __ldg(a.src + e) * (__ldg(a.wgt + e) * a.wscale);
   } else {
     // r = (y - A x) / rowSum where rowSum != 0, else A x (AAPM_script/OSSART_AAPM.m:86-88),
     // times the channel weight

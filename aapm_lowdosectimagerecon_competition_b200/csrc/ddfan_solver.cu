@@ -605,7 +605,7 @@ static int solver_weights(Solver& s, const PlanDesc& d, const std::vector<float>
   PsScanArgs q{};
   q.tab = sq.p; q.nlines = (int)R; q.N = DNU; q.Nw = DNU + 1; q.src = sino.p; q.lines_per_slice = 1;
   q.wgt = cvd.p; q.wscale = 1.f;
-  if ((rc = ps_scan(p.mode, 0, q, st))) return rc;
+  if ((rc = ps_scan(p.mode, 2, q, st))) return rc;
   PsBackArgs b{};
   b.sq = sq.p; b.vg = vg.p; b.fc = fc.p;
   b.tb = p.d_tb; b.lut = p.d_lut; b.t0 = p.t0; b.invdt = p.invdt; b.dirt = p.dirt; b.M = p.M;
