@@ -10,9 +10,9 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libddfan.so")
 
 OK = 0
-SAT_FP32, SAT_HILO, SAT_FP64 = 0, 1, 2
+SAT_FP32, SAT_HILO, SAT_FP64, SAT_DIRECT = 0, 1, 2, 3
 BACK_REF, BACK_ADJ = 0, 1
-SAT_MODES = {"fp32": SAT_FP32, "hilo": SAT_HILO, "fp64": SAT_FP64}
+SAT_MODES = {"fp32": SAT_FP32, "hilo": SAT_HILO, "fp64": SAT_FP64, "direct": SAT_DIRECT}
 BACK_MODES = {"ref": BACK_REF, "adj": BACK_ADJ}
 
 _f = ctypes.c_float

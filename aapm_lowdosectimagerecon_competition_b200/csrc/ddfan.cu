@@ -99,6 +99,16 @@ int pow2_zl(int ZB) {
   return best;
 }
 
+int plan_zl(int ZB, int zl_force) {
+  int ZL = pow2_zl(ZB);
+  if (const char* zl = getenv("DDFAN_ZL")) {
+    const int v = atoi(zl);
+    if ((v == 1 || v == 2 || v == 4 || v == 8) && v <= ZL) ZL = v;
+  }
+  if (zl_force == 1 || zl_force == 2 || zl_force == 4 || zl_force == 8) ZL = zl_force;
+  return ZL;
+}
+
 // Stream-ordered device memory from one pool per device owned by the
 // library: creating or destroying a plan or a solver never synchronises the
 // device, so other solves keep running meanwhile.  The pool keeps the blocks
@@ -216,7 +226,7 @@ int plan_create(Plan** out, const PlanDesc& d) {
     return set_err(DDFAN_ERR_ARG, "plan: bad sizes (DNU=%d XN=%d YN=%d SLN=%d PNmax=%d) or null geometry",
                    d.DNU, d.XN, d.YN, d.SLN, d.PNmax);
   if (!(d.dx > 0.f)) return set_err(DDFAN_ERR_ARG, "plan: dx must be > 0");
-  if (d.sat_mode < SAT_FP32 || d.sat_mode > SAT_FP64) return set_err(DDFAN_ERR_ARG, "plan: sat_mode %d", d.sat_mode);
+  if (d.sat_mode < SAT_FP32 || d.sat_mode > SAT_DIRECT) return set_err(DDFAN_ERR_ARG, "plan: sat_mode %d", d.sat_mode);
   if (d.XN > 1024 || d.YN > 1024 || d.DNU + 1 > 1024)
     return set_err(DDFAN_ERR_UNSUPPORTED, "plan: lines longer than 1024 cells are not supported");
   int ndev = 0;
@@ -232,13 +242,11 @@ int plan_create(Plan** out, const PlanDesc& d) {
   Plan& p = *P;
   p.device = d.device;
   p.XN = d.XN; p.YN = d.YN; p.U = d.DNU; p.Z = d.SLN; p.ZB = (d.SLN + 3) / 4;
-  p.PNmax = d.PNmax; p.mode = d.sat_mode; p.ZL = pow2_zl(p.ZB);
-  if (const char* zl = getenv("DDFAN_ZL")) {
-    const int v = atoi(zl);
-    if ((v == 1 || v == 2 || v == 4 || v == 8) && v <= p.ZL) p.ZL = v;
-  }
-  if (d.zl_force == 1 || d.zl_force == 2 || d.zl_force == 4 || d.zl_force == 8) p.ZL = d.zl_force;
-  p.ZB = (p.ZB + p.ZL - 1) / p.ZL * p.ZL;  // whole z-tiles (padding blocks hold zeros)
+  p.PNmax = d.PNmax; p.mode = d.sat_mode; p.ZL = plan_zl(p.ZB, d.zl_force);
+  p.P4 = p.ZB;
+  // whole z-tiles: the padding blocks of the last tile are never written; the
+  // projectors read them only for the slices past Z, whose results they drop
+  p.ZB = (p.ZB + p.ZL - 1) / p.ZL * p.ZL;
   p.x0 = d.x0; p.y0 = d.y0; p.dx = d.dx; p.detCntIdx = d.detCntIdx;
   p.ocx = (d.XN - 1.0) * 0.5 - (double)d.imgXCenter / (double)d.dx;
   p.ocy = (d.YN - 1.0) * 0.5 - (double)d.imgYCenter / (double)d.dx;
@@ -293,17 +301,21 @@ int plan_create(Plan** out, const PlanDesc& d) {
     return set_err(DDFAN_ERR_CUDA, "plan: stream/event creation failed");
   }
   cudaStream_t as = p.alloc_stream;
+  const bool direct = p.mode == SAT_DIRECT;
   const size_t F4 = cell_f4(p.mode);
-  const size_t nimg = (size_t)p.XN * p.YN * p.ZB * F4;
-  const size_t nsino = (size_t)p.PNmax * (p.U + 1) * p.ZB * F4;
+  // direct mode: no image tables; the staged sinogram operand [PNmax][U+1][P4]
+  // float4 and a staged image of 4 P4 slices
+  const size_t nimg = direct ? 0 : (size_t)p.XN * p.YN * p.ZB * F4;
+  const size_t nsino = direct ? (size_t)p.PNmax * (p.U + 1) * p.P4 : (size_t)p.PNmax * (p.U + 1) * p.ZB * F4;
+  const size_t ntmp = (size_t)p.XN * p.YN * (direct ? 4 * (size_t)p.P4 : (size_t)p.Z);
   if ((rc = dalloc(&p.d_bx, p.U + 1, &B, as)) || (rc = dalloc(&p.d_by, p.U + 1, &B, as)) ||
       (rc = dalloc(&p.d_xd, p.U, &B, as)) || (rc = dalloc(&p.d_yd, p.U, &B, as)) ||
       (rc = dalloc(&p.d_mask, (size_t)p.XN * p.YN, &B, as)) || (rc = dalloc(&p.d_tb, p.U + 1, &B, as)) ||
-      (rc = dalloc(&p.d_lut, p.M, &B, as)) || (rc = dalloc(&p.d_satx, nimg, &B, as)) ||
-      (rc = dalloc(&p.d_saty, nimg, &B, as)) || (rc = dalloc(&p.d_satq, nsino, &B, as)) ||
+      (rc = dalloc(&p.d_lut, p.M, &B, as)) || (!direct && (rc = dalloc(&p.d_satx, nimg, &B, as))) ||
+      (!direct && (rc = dalloc(&p.d_saty, nimg, &B, as))) || (rc = dalloc(&p.d_satq, nsino, &B, as)) ||
       (rc = dalloc(&p.d_vg, p.PNmax, &B, as)) || (rc = dalloc(&p.d_fc, (size_t)p.PNmax * (p.U + 1), &B, as)) ||
       (rc = dalloc(&p.d_cvd, (size_t)p.PNmax * p.U, &B, as)) ||
-      (rc = dalloc(&p.d_tmp, (size_t)p.XN * p.YN * p.Z, &B, as)) ||
+      (rc = dalloc(&p.d_tmp, ntmp, &B, as)) ||
       (rc = dalloc(&p.d_angs, (size_t)p.PNmax, &B, as)) ||
       (rc = dalloc(&p.d_order, (size_t)p.PNmax, &B, as)) || (rc = dalloc(&p.d_counts, 2, &B, as))) {
     if (prev >= 0) cudaSetDevice(prev);
@@ -585,6 +597,146 @@ int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2*
   return check_launch("k_back_adj<y>");
 }
 
+// ------------------------------------------------------------------ direct mode
+
+static int grid_blocks(size_t n) { return (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 148 * 16)); }
+
+int launch_stage_image(const float* src, int Z, const uint8_t* mask, float* dst, int Zp, size_t npix,
+                       cudaStream_t st) {
+  k_stage_image<<<grid_blocks(npix * Zp), 256, 0, st>>>(src, Z, mask, dst, Zp, npix);
+  return check_launch("k_stage_image");
+}
+
+int launch_stage_sino(const float* src, int Z, const float* wgt, int U, float* dst, int Zp, size_t PN,
+                      cudaStream_t st) {
+  ProfScope ps(KIND_SAT_SINO, st);
+  k_stage_sino<<<grid_blocks(PN * (U + 1) * Zp), 256, 0, st>>>(src, Z, wgt, U, dst, Zp, PN);
+  return check_launch("k_stage_sino");
+}
+
+int launch_publish_masked(const float* x, int Zi, const float* x0, int Z, const uint8_t* mask, int clamp0,
+                          float* out, size_t npix, cudaStream_t st) {
+  k_publish_masked<<<grid_blocks(npix * Z), 256, 0, st>>>(x, Zi, x0, Z, mask, clamp0, out, npix);
+  return check_launch("k_publish_masked");
+}
+
+template <int ZL>
+static void fwd_dd_go(const DdFwdArgs& a, int nzt, cudaStream_t st) {
+  constexpr int CG = FwdCG<ZL>::v;
+  using T = DdFwdTile<ZL, CG>;
+  constexpr int kMaxRows = 65535;  // grid y limit
+  for (int r0 = 0; r0 < a.PN; r0 += kMaxRows) {
+    DdFwdArgs b = a;
+    b.row0 = r0;
+    dim3 grid((a.U + T::CW - 1) / T::CW, std::min(a.PN - r0, kMaxRows), nzt);
+    k_fwd_dd<ZL, CG><<<grid, T::NT, 0, st>>>(b);
+  }
+}
+
+int launch_fwd_dd(const Plan& p, const float* img, const ViewGeom* vg, const double2* fc, const float* cvd,
+                  const int* order, int PN, float* out, int orow, int ostride, int zlo, int zhi,
+                  const DdResidual* res, cudaStream_t st) {
+  DdFwdArgs a{};
+  a.img = reinterpret_cast<const float4*>(img); a.P4 = p.P4;
+  a.vg = vg; a.fc = fc; a.cvd = cvd; a.order = order;
+  a.out = out; a.orow = orow; a.ostride = ostride;
+  a.PN = PN; a.U = p.U; a.Z = p.Z; a.XN = p.XN; a.YN = p.YN; a.dx = (float)p.dx;
+  a.zlo = zlo; a.zhi = zhi < 0 ? p.Z : zhi; a.row0 = 0;
+  if (res) {
+    a.y = res->y; a.yview = res->yview; a.rowsum = res->rowsum; a.wgt = res->wgt; a.ystride = res->ystride;
+  }
+  int nzt = 0;
+  ztile_range(p, zlo, zhi, &a.zt0, &nzt);
+  if (nzt == 0 || PN < 1) return DDFAN_OK;
+  ProfScope ps(KIND_FWD, st);
+  switch (p.ZL) {
+    case 8: fwd_dd_go<8>(a, nzt, st); break;
+    case 4: fwd_dd_go<4>(a, nzt, st); break;
+    case 2: fwd_dd_go<2>(a, nzt, st); break;
+    default: fwd_dd_go<1>(a, nzt, st); break;
+  }
+  return check_launch("k_fwd_dd");
+}
+
+template <int ZL, bool XM>
+static void back_dd_go(const DdAdjArgs& a, int nzt, cudaStream_t st) {
+  using T = BackTile<ZL>;
+  const int nl = XM ? a.XN : a.YN, N = XM ? a.YN : a.XN;
+  const int tiles = ((nl + T::LT - 1) / T::LT) * ((N + T::KT - 1) / T::KT);
+  k_back_dd<ZL, XM><<<dim3(tiles, 1, nzt), T::NT, 0, st>>>(a);
+}
+
+template <bool XM>
+static void back_dd_zl(int ZL, const DdAdjArgs& a, int nzt, cudaStream_t st) {
+  switch (ZL) {
+    case 8: back_dd_go<8, XM>(a, nzt, st); break;
+    case 4: back_dd_go<4, XM>(a, nzt, st); break;
+    case 2: back_dd_go<2, XM>(a, nzt, st); break;
+    default: back_dd_go<1, XM>(a, nzt, st); break;
+  }
+}
+
+template <int ZL>
+static void ref_dd_go(const DdRefArgs& a, int nzt, cudaStream_t st) {
+  using T = BackTile<ZL>;
+  const int tiles = ((a.YN + T::LT - 1) / T::LT) * ((a.XN + T::KT - 1) / T::KT);
+  k_back_ref_dd<ZL><<<dim3(tiles, 1, nzt), T::NT, 0, st>>>(a);
+}
+
+int launch_back_dd(const Plan& p, int back_mode, const float* w, const ViewGeom* vg, const double2* fc,
+                   const int* order, const int* counts, int PN, const BackEpi& epi, cudaStream_t st) {
+  int zt0 = 0, nzt = 0;
+  ztile_range(p, epi.zlo, epi.zhi, &zt0, &nzt);
+  if (nzt == 0 || PN < 1) return DDFAN_OK;
+  if (back_mode == DDFAN_BACK_REF) {
+    DdRefArgs a{};
+    a.q = reinterpret_cast<const float4*>(w); a.P4 = p.P4; a.vg = vg;
+    a.PN = PN; a.U = p.U; a.Z = p.Z; a.XN = p.XN; a.YN = p.YN;
+    a.ocx = p.ocx; a.ocy = p.ocy; a.dx = p.dx;
+    a.inv_sid = p.inv_sid; a.inv_dbeta = p.inv_dbeta; a.cnt = (double)p.detCntIdx + 0.5;
+    a.epi = epi;
+    a.zt0 = zt0;
+    ProfScope ps(KIND_BACK_A, st);
+    switch (p.ZL) {
+      case 8: ref_dd_go<8>(a, nzt, st); break;
+      case 4: ref_dd_go<4>(a, nzt, st); break;
+      case 2: ref_dd_go<2>(a, nzt, st); break;
+      default: ref_dd_go<1>(a, nzt, st); break;
+    }
+    return check_launch("k_back_ref_dd");
+  }
+  if (back_mode != DDFAN_BACK_ADJ) return set_err(DDFAN_ERR_ARG, "back_mode %d", back_mode);
+  if (!p.adj_ok) return set_err(DDFAN_ERR_UNSUPPORTED, "detector boundaries are not monotone as seen from the source");
+  if (!order || !counts) return set_err(DDFAN_ERR_ARG, "exact adjoint needs the view order");
+  if (p.U + 1 > 1024 || p.M > 4096) return set_err(DDFAN_ERR_UNSUPPORTED, "exact adjoint: %d channels", p.U);
+  DdAdjArgs a{};
+  a.w = reinterpret_cast<const float4*>(w); a.P4 = p.P4;
+  a.vg = vg; a.fc = fc; a.tb = p.d_tb; a.lut = p.d_lut;
+  a.order = order; a.counts = counts;
+  a.t0 = p.t0; a.invdt = p.invdt; a.dirt = p.dirt; a.M = p.M;
+  a.PN = PN; a.U = p.U; a.Z = p.Z; a.XN = p.XN; a.YN = p.YN;
+  a.ocx = p.ocx; a.ocy = p.ocy; a.dx = p.dx;
+  a.zt0 = zt0;
+  // pass 1: x-major views along x columns -> tmp (mask applied)
+  a.epi = epi;
+  a.epi.out = p.d_tmp; a.epi.addend = nullptr; a.epi.xin = nullptr; a.epi.colsum = nullptr;
+  a.epi.nonneg = 0;
+  {
+    ProfScope ps(KIND_BACK_A, st);
+    back_dd_zl<true>(p.ZL, a, nzt, st);
+  }
+  int rc = check_launch("k_back_dd<x>");
+  if (rc) return rc;
+  // pass 2: y-major views along y rows, plus pass 1, then the final epilogue
+  a.epi = epi;
+  a.epi.addend = p.d_tmp;
+  {
+    ProfScope ps(KIND_BACK_B, st);
+    back_dd_zl<false>(p.ZL, a, nzt, st);
+  }
+  return check_launch("k_back_dd<y>");
+}
+
 // ------------------------------------------------------------------ device API
 
 int proj_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const float* d_vol, float* d_prj,
@@ -592,6 +744,20 @@ int proj_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const floa
   int rc;
   if ((rc = launch_view_geom(p, d_angs, stride, PN, p.d_vg, p.d_fc, p.d_cvd, st))) return rc;
   if ((rc = launch_view_order(p.d_vg, PN, p.d_order, p.d_counts, st))) return rc;
+  if (p.mode == SAT_DIRECT) {
+    // the kernel reads 4-slice float4 runs of a masked image: stage the
+    // caller's image unless it already is one
+    const float* img = d_vol;
+    if (p.has_mask || (p.Z & 3) || (reinterpret_cast<uintptr_t>(d_vol) & 15)) {
+      if ((rc = launch_stage_image(d_vol, p.Z, p.has_mask ? p.d_mask : nullptr, p.d_tmp, 4 * p.P4,
+                                   (size_t)p.XN * p.YN, st)))
+        return rc;
+      img = p.d_tmp;
+    }
+    rc = launch_fwd_dd(p, img, p.d_vg, p.d_fc, p.d_cvd, p.d_order, PN, d_prj, p.U, p.Z, zlo, zhi, nullptr, st);
+    mark_use(p, st);
+    return rc;
+  }
   if ((rc = launch_sat_image(p, d_vol, st, zlo, zhi))) return rc;
   rc = launch_fwd(p, p.d_vg, p.d_fc, p.d_cvd, p.d_order, PN, d_prj, zlo, zhi, st);
   mark_use(p, st);
@@ -604,11 +770,18 @@ int back_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const floa
   if ((rc = launch_view_geom(p, d_angs, stride, PN, p.d_vg, p.d_fc, p.d_cvd, st))) return rc;
   if ((rc = launch_view_order(p.d_vg, PN, p.d_order, p.d_counts, st))) return rc;
   const bool adj = back_mode == DDFAN_BACK_ADJ;
+  BackEpi e{};
+  e.out = d_vol; e.mask = p.has_mask ? p.d_mask : nullptr; e.zlo = zlo; e.zhi = zhi;
+  if (p.mode == SAT_DIRECT) {
+    float* w = reinterpret_cast<float*>(p.d_satq);
+    if ((rc = launch_stage_sino(d_prj, p.Z, adj ? p.d_cvd : nullptr, p.U, w, 4 * p.P4, (size_t)PN, st))) return rc;
+    rc = launch_back_dd(p, back_mode, w, p.d_vg, p.d_fc, p.d_order, p.d_counts, PN, e, st);
+    mark_use(p, st);
+    return rc;
+  }
   if ((rc = launch_sat_sino(p, d_prj, PN, adj ? p.d_cvd : nullptr, 1.f, nullptr, nullptr, nullptr, st, zlo,
                             zhi)))
     return rc;
-  BackEpi e{};
-  e.out = d_vol; e.mask = p.has_mask ? p.d_mask : nullptr; e.zlo = zlo; e.zhi = zhi;
   rc = launch_back(p, back_mode, p.d_vg, p.d_fc, p.d_order, p.d_counts, PN, e, st);
   mark_use(p, st);
   return rc;
@@ -830,15 +1003,18 @@ DDFAN_API int ddfan_tune_set_zl(int zblocks, int zl) {
 DDFAN_API int ddfan_tune_get_zl(int zblocks) { return zblocks < 1 ? 0 : pow2_zl(zblocks); }
 
 DDFAN_API size_t ddfan_plan_estimate_bytes(int XN, int YN, int DNU, int SLN, int PNmax, int sat_mode) {
-  if (XN < 1 || YN < 1 || DNU < 2 || SLN < 1 || PNmax < 1 || sat_mode < 0 || sat_mode > 2) return 0;
-  int ZB = (SLN + 3) / 4;
+  if (XN < 1 || YN < 1 || DNU < 2 || SLN < 1 || PNmax < 1 || sat_mode < 0 || sat_mode > SAT_DIRECT) return 0;
+  const int P4 = (SLN + 3) / 4;
+  int ZB = P4;
   const int ZL = pow2_zl(ZB);
   ZB = (ZB + ZL - 1) / ZL * ZL;
   const size_t F4 = cell_f4(sat_mode), U = (size_t)DNU, P = (size_t)PNmax;
-  const size_t cells = 2 * (size_t)XN * YN * ZB * F4 + P * (U + 1) * ZB * F4;
+  const bool direct = sat_mode == SAT_DIRECT;
+  const size_t cells = direct ? P * (U + 1) * P4 : 2 * (size_t)XN * YN * ZB * F4 + P * (U + 1) * ZB * F4;
+  const size_t tmp = (size_t)XN * YN * (direct ? 4 * (size_t)P4 : (size_t)SLN);
   return cells * sizeof(float4) + (2 * (U + 1) + 2 * U) * sizeof(double) + (size_t)XN * YN +
          (U + 1) * sizeof(float) + 4 * (U + 1) * sizeof(uint16_t) + P * sizeof(ViewGeom) +
-         P * (U + 1) * sizeof(double2) + P * U * sizeof(float) + (size_t)XN * YN * SLN * sizeof(float) +
+         P * (U + 1) * sizeof(double2) + P * U * sizeof(float) + tmp * sizeof(float) +
          P * sizeof(float) + P * sizeof(int) + 2 * sizeof(int);
 }
 

@@ -1,0 +1,496 @@
+// ddfan_dd_kernels.cuh -- projector kernels that read the values themselves
+// instead of prefix-sum tables (DDFAN_SAT_DIRECT).
+//
+// Every sample of the branchless DD path is a difference of two linearly
+// interpolated prefix sums, Phi(c1) - Phi(c0), with Phi(c) = S[k] + f v[k]
+// (k = floor of the clamped c, f its fraction; AAPM_script/
+// MultiSlicesProjGPU.cu:161-170, MultiSlicesBackGPU.cu:175-179).  The
+// difference telescopes to the values between the two positions:
+//   k1 == k0:  (f1 - f0) v[k0]
+//   k1 >  k0:  (1 - f0) v[k0] + sum_{k0<k<k1} v[k] + f1 v[k1]
+//   k1 <  k0:  -f0 v[k0] - sum_{k1<k<k0} v[k] + (f1 - 1) v[k1]
+// -- the same number in exact arithmetic, with no cancellation in FP32 and
+// without building or reading a table.  A DD footprint covers one to three
+// values at the geometries this path serves (the axis is chosen so that a ray
+// crosses at most one cell per line, and channel and pixel pitch are
+// comparable), so a sample reads one float per slice plus the one it shares
+// with its neighbour, where a 48-byte hi/lo cell read 12 bytes per slice per
+// boundary.  Wider footprints walk more values (any width is correct).
+//
+// Layouts: the image [YN][XN][P4] float4 (4 slices per float4, P4 = padded
+// slices / 4) is read straight, masked beforehand; the sinogram operands
+// [slot][U + 1][P4] float4 hold the (weighted) residual with a zero guard
+// channel U, so a walk that ends on the last boundary (index U, fraction 0)
+// reads a zero.  Geometry phases (FP64 boundary lines, brackets, fractions)
+// are those of the prefix-sum kernels; only the gather changes.
+#pragma once
+#include "ddfan_proj_kernels.cuh"
+
+namespace ddfan {
+
+#ifndef DDFAN_DD_FWD_MIN_CTAS
+#define DDFAN_DD_FWD_MIN_CTAS 3
+#endif
+#ifndef DDFAN_DD_BACK_MIN_CTAS
+#define DDFAN_DD_BACK_MIN_CTAS 4
+#endif
+
+__device__ __forceinline__ void fma4(float (&a)[4], float w, const float4& v) {
+  a[0] = fmaf(w, v.x, a[0]);
+  a[1] = fmaf(w, v.y, a[1]);
+  a[2] = fmaf(w, v.z, a[2]);
+  a[3] = fmaf(w, v.w, a[3]);
+}
+
+// Weights of the telescoped difference from (k0, f0) to (k1, f1), scaled by
+// `s`: value = w0 v[k0] + wi sum(interior) + we v[k1].
+__device__ __forceinline__ float3 walk_weights(int k0, float f0, int k1, float f1, float s) {
+  if (k1 == k0) return make_float3((f1 - f0) * s, 0.f, 0.f);
+  if (k1 > k0) return make_float3((1.f - f0) * s, s, f1 * s);
+  return make_float3(-f0 * s, -s, (f1 - 1.f) * s);
+}
+
+// ============================================================ forward projector
+
+struct DdFwdArgs {
+  const float4* img;   // masked image [YN][XN][P4]
+  int P4;
+  const ViewGeom* vg;
+  const double2* fc;   // [PN][U+1] boundary lines
+  const float* cvd;    // [PN][U] 1 / |dir.axis|
+  const int* order;    // CTA row -> view, x-major first (null = identity)
+  float* out;          // [slot][orow][ostride]
+  int orow, ostride;
+  int PN, U, Z, XN, YN;
+  float dx;
+  int zlo, zhi, zt0, row0;
+  // fused OS-SART residual (AAPM_script/OSSART_AAPM.m:86-88); y null = plain projection
+  const float* y;      // measured [views][U][ystride]
+  const int* yview;    // slot -> measured view
+  const float* rowsum; // [slot][U]
+  const float* wgt;    // [slot][U] weight of the exact adjoint, or null
+  int ystride;
+};
+
+template <int ZL, int CG>
+struct DdFwdTile {
+  static constexpr int NT = 256;
+  static constexpr int NG = NT / ZL;     // channel groups
+  static constexpr int CW = NG * CG;     // channels per CTA
+  static constexpr int NB = CW + 1;
+  static constexpr int CC = 2048 / CW;   // lines per geometry chunk
+};
+
+// CTA = one view x CW channels x 4*ZL slices; a thread owns CG consecutive
+// channels x 4 slices and walks their footprints along each line, carrying
+// the value at the boundary two channels share.  Phase G (per chunk of CC
+// lines): for each channel the cell index of its first boundary and the walk
+// weights over 1 / footprint length (MultiSlicesProjGPU.cu:166-170).
+template <int ZL, int CG>
+__global__ void __launch_bounds__(256, DDFAN_DD_FWD_MIN_CTAS) k_fwd_dd(DdFwdArgs a) {
+  using T = DdFwdTile<ZL, CG>;
+  constexpr int NT = T::NT, CW = T::CW, NB = T::NB, CC = T::CC;
+  __shared__ double2 s_fc[NB];
+  __shared__ int s_k[CC][CW];
+  __shared__ float4 s_w[CC][CW];  // (w0, wi, we) / length, step count as int bits
+  const int tid = threadIdx.x;
+  const int zl = tid % ZL, g = tid / ZL;
+  const int zt = blockIdx.z + a.zt0;
+  const int row = a.row0 + (int)blockIdx.y;
+  if (row >= a.PN) return;  // uniform per CTA
+  const int slot = a.order ? a.order[row] : row;
+  const int p = slot;
+  const int zb = zt * ZL + zl;
+  const int ub0 = blockIdx.x * CW;
+  const bool xm = a.vg[p].xmajor != 0;
+  const int nl = xm ? a.XN : a.YN, N = xm ? a.YN : a.XN;
+  for (int b = tid; b < NB; b += NT) s_fc[b] = a.fc[(size_t)p * (a.U + 1) + min(ub0 + b, a.U)];
+  const bool active = (ub0 + g * CG < a.U) && (zb < a.P4);
+  // x-major views integrate along x columns (line = x, k = y), the others along y rows
+  const size_t P4 = (size_t)a.P4;
+  const size_t kstride = (xm ? (size_t)a.XN : 1) * P4;
+  const size_t lstride = (xm ? 1 : (size_t)a.XN) * P4;
+  const float4* img = a.img + (active ? zb : 0);
+  float acc[CG][4];
+#pragma unroll
+  for (int j = 0; j < CG; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+  const double Nd = (double)N;
+  const float dx = a.dx;
+  __syncthreads();
+  for (int ii0 = 0; ii0 < nl; ii0 += CC) {
+    for (int e = tid; e < CC * CW; e += NT) {
+      const int col = e / CW, j = e - col * CW;
+      const double di = (double)(ii0 + col);
+      const double2 fa = s_fc[j], fb = s_fc[j + 1];
+      const double c0 = fma(di, fa.x, fa.y), c1 = fma(di, fb.x, fb.y);
+      const double cc0 = fmin(fmax(c0, 0.0), Nd), cc1 = fmin(fmax(c1, 0.0), Nd);
+      const int k0 = min((int)cc0, N - 1), k1 = min((int)cc1, N - 1);
+      const float f0 = (float)(cc0 - (double)k0), f1 = (float)(cc1 - (double)k1);
+      const float inv = ub0 + j < a.U ? __frcp_rn((float)(c1 - c0) * dx) : 0.f;
+      const float3 w = walk_weights(k0, f0, k1, f1, inv);
+      s_k[col][j] = k0;
+      s_w[col][j] = make_float4(w.x, w.y, w.z, __int_as_float(k1 - k0));
+    }
+    __syncthreads();
+    if (active) {
+      const int ncol = min(CC, nl - ii0);
+      float part[CG][4];
+#pragma unroll
+      for (int j = 0; j < CG; ++j) part[j][0] = part[j][1] = part[j][2] = part[j][3] = 0.f;
+      for (int col = 0; col < ncol; ++col) {
+        const float4* line = img + (size_t)(ii0 + col) * lstride;
+        int k = s_k[col][g * CG];
+        float4 cur = __ldg(line + (size_t)k * kstride);
+#pragma unroll
+        for (int j = 0; j < CG; ++j) {
+          const float4 w = s_w[col][g * CG + j];
+          const int dn = __float_as_int(w.w);
+          fma4(part[j], w.x, cur);
+          if (dn != 0) {
+            const int st = dn > 0 ? 1 : -1, n = dn > 0 ? dn : -dn;
+            for (int i = 1; i < n; ++i) fma4(part[j], w.y, __ldg(line + (size_t)(k + i * st) * kstride));
+            k += dn;
+            cur = __ldg(line + (size_t)k * kstride);
+            fma4(part[j], w.z, cur);
+          }
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < CG; ++j)
+#pragma unroll
+        for (int s = 0; s < 4; ++s) acc[j][s] += part[j][s];
+    }
+    __syncthreads();
+  }
+  if (!active) return;
+#pragma unroll
+  for (int j = 0; j < CG; ++j) {
+    const int u = ub0 + g * CG + j;
+    if (u >= a.U) break;
+    const size_t e = (size_t)slot * a.U + u;
+    const float cv = __ldg(a.cvd + e) * dx;
+    float* o = a.out + ((size_t)slot * a.orow + u) * a.ostride;
+    float rs = 0.f, wt = 1.f;
+    const float* yv = nullptr;
+    if (a.y) {
+      rs = __ldg(a.rowsum + e);
+      if (a.wgt) wt = __ldg(a.wgt + e);
+      yv = a.y + ((size_t)__ldg(a.yview + slot) * a.U + u) * a.ystride;
+    }
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const int z = zb * 4 + s;
+      if (z < a.zlo || z >= a.zhi) continue;
+      float val = acc[j][s] * cv;
+      if (yv) {
+        // (y - A x) / rowSum where rowSum != 0, else A x (AAPM_script/OSSART_AAPM.m:88)
+        val = rs != 0.f ? __fdiv_rn(__fsub_rn(__ldg(yv + z), val), rs) : val;
+        val *= wt;
+      }
+      o[z] = val;
+    }
+  }
+}
+
+// ============================================================ exact adjoint
+
+struct DdAdjArgs {
+  const float4* w;      // weighted residual [slot][U+1][P4], r_u / |dir_u.axis|, channel U = 0
+  int P4;
+  const ViewGeom* vg;
+  const double2* fc;
+  const float* tb;
+  const uint16_t* lut;
+  const int* order;
+  const int* counts;
+  float t0, invdt, dirt;
+  int M;
+  int PN, U, Z, XN, YN;
+  double ocx, ocy, dx;
+  BackEpi epi;
+  int zt0;
+};
+
+// Transpose of k_fwd_dd, on the geometry of k_back_adj: pixel k of line ii
+// receives sum_u w_u (fraction of footprint u inside [k, k+1]) = Q(beta(k+1))
+// - Q(beta(k)), Q the channel prefix sum of w, beta the fractional boundary
+// index of a pixel edge (bracket from the fan-tangent table, fraction from the
+// FP64 boundary lines).  Here the difference is walked over w itself; a
+// thread owns VG consecutive pixels of a line, whose walks chain (the end of
+// one is the start of the next).
+template <int ZL, bool XM>
+__global__ void __launch_bounds__(256, DDFAN_DD_BACK_MIN_CTAS) k_back_dd(DdAdjArgs a) {
+  using T = BackTile<ZL>;
+  constexpr int NT = T::NT, VG = T::VG, SPL = T::SPL, KT = T::KT, LT = T::LT, NE = T::NE;
+  constexpr int LS = T::LS, NES = T::NES;
+  constexpr int VC = (1024 / NE) < 1 ? 1 : ((1024 / NE) > 4 ? 4 : 1024 / NE);
+  constexpr int TBMAX = 1024, LUTMAX = 4096;
+  __shared__ int2 s_geo[VC][NES];  // edge k of line l at l * LS + k + k / VG
+  __shared__ int s_p[VC];
+  __shared__ float s_sgn[VC];
+  __shared__ float s_tb[TBMAX];
+  __shared__ uint16_t s_lut[LUTMAX];
+  const int tid = threadIdx.x;
+  const int zl = tid % ZL, g = tid / ZL;
+  const int zt = blockIdx.z + a.zt0;
+  const int zb = zt * ZL + zl;
+  const int nl = XM ? a.XN : a.YN, N = XM ? a.YN : a.XN;
+  const int ntk = (N + KT - 1) / KT;
+  const int tl = blockIdx.x / ntk, tk = blockIdx.x - tl * ntk;
+  const int l0 = tl * LT, k0 = tk * KT;
+  const int l = g / SPL, sg = g - l * SPL;
+  const int ii = l0 + l, ks = k0 + sg * VG;
+  const bool active = zb < a.P4 && ii < nl && ks < N;
+  for (int i = tid; i <= a.U; i += NT) s_tb[i] = a.tb[i];
+  for (int i = tid; i < a.M; i += NT) s_lut[i] = a.lut[i];
+  const int nx = a.counts[0];
+  const int vbeg = XM ? 0 : nx, vend = XM ? nx : a.PN;
+  float acc[VG][4];
+#pragma unroll
+  for (int v = 0; v < VG; ++v) acc[v][0] = acc[v][1] = acc[v][2] = acc[v][3] = 0.f;
+  const size_t P4 = (size_t)a.P4;
+  const size_t vstride = (size_t)(a.U + 1) * P4;
+  const double ocl = XM ? a.ocx : a.ocy, ock = XM ? a.ocy : a.ocx;
+  __syncthreads();
+  const float tfirst = s_tb[0], tlast = s_tb[a.U];
+  for (int v0 = vbeg; v0 < vend; v0 += VC) {
+    const int nvc = min(VC, vend - v0);
+    if (tid < VC && tid < nvc) {
+      const int p = a.order[v0 + tid];
+      s_p[tid] = p;
+      s_sgn[tid] = a.vg[p].sgn;
+    }
+    for (int e = tid; e < VC * NE; e += NT) {
+      const int vv = e / NE, r = e - vv * NE;
+      const int le = r / (KT + 1), ke = r - le * (KT + 1);
+      const int li = l0 + le, ck = k0 + ke;
+      int b = 0;
+      float frac = 0.f;
+      if (vv < nvc && li < nl && ck <= N) {
+        const int p = a.order[v0 + vv];
+        const ViewGeom& G = a.vg[p];
+        const double lineX = (li - ocl) * a.dx, along = ((double)ck - 0.5 - ock) * a.dx;
+        const float vx = (float)((XM ? lineX : along) - G.sx);
+        const float vy = (float)((XM ? along : lineX) - G.sy);
+        const float cr = G.shx * vy - G.shy * vx, dt = G.shx * vx + G.shy * vy;
+        const float t = a.dirt * __fdividef(cr, dt);
+        if (!(t >= tfirst)) {
+          b = 0;
+        } else if (t >= tlast) {
+          b = a.U;
+        } else {
+          const int m = (int)fminf(fmaxf((t - a.t0) * a.invdt, 0.f), (float)(a.M - 1));
+          b = s_lut[m];
+          int guard = 0;
+          while (b < a.U - 1 && s_tb[b + 1] <= t && guard++ < 64) ++b;
+          while (b > 0 && s_tb[b] > t && guard++ < 128) --b;
+          const double2* fcp = a.fc + (size_t)p * (a.U + 1);
+          const double2 f0 = __ldg(fcp + b), f1 = __ldg(fcp + b + 1);
+          const double di = (double)li;
+          const double c0 = fma(di, f0.x, f0.y), c1 = fma(di, f1.x, f1.y);
+          frac = __fdiv_rn((float)((double)ck - c0), (float)(c1 - c0));
+          frac = fminf(fmaxf(frac, 0.f), 1.f);
+        }
+      }
+      s_geo[vv][le * LS + ke + ke / VG] = make_int2(b, __float_as_int(frac));
+    }
+    __syncthreads();
+    if (active) {
+      for (int vv = 0; vv < nvc; ++vv) {
+        const float4* base = a.w + (size_t)s_p[vv] * vstride + zb;
+        const float sgn = s_sgn[vv];
+        const int2* geo = &s_geo[vv][l * LS + sg * (VG + 1)];
+        int2 gi = geo[0];
+        int k = gi.x;
+        float f = __int_as_float(gi.y);
+        float4 cur = __ldg(base + (size_t)k * P4);
+#pragma unroll
+        for (int v = 0; v < VG; ++v) {
+          gi = geo[v + 1 == VG ? VG + 1 : v + 1];
+          const int k1 = gi.x;
+          const float f1 = __int_as_float(gi.y);
+          const float3 w = walk_weights(k, f, k1, f1, sgn);
+          fma4(acc[v], w.x, cur);
+          const int dn = k1 - k;
+          if (dn != 0) {
+            const int st = dn > 0 ? 1 : -1, n = dn > 0 ? dn : -dn;
+            for (int i = 1; i < n; ++i) fma4(acc[v], w.y, __ldg(base + (size_t)(k + i * st) * P4));
+            k = k1;
+            cur = __ldg(base + (size_t)k * P4);
+            fma4(acc[v], w.z, cur);
+          }
+          f = f1;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (!active) return;
+#pragma unroll
+  for (int v = 0; v < VG; ++v) {
+    const int kk = ks + v;
+    if (kk >= N) break;
+    back_store(a.epi, XM ? ii : kk, XM ? kk : ii, zb, a.XN, a.Z, true, acc[v]);
+  }
+}
+
+// ============================================================ reference backprojector
+
+struct DdRefArgs {
+  const float4* q;     // residual [slot][U+1][P4] (unweighted), channel U = 0
+  int P4;
+  const ViewGeom* vg;
+  int PN, U, Z, XN, YN;
+  double ocx, ocy, dx, inv_sid, inv_dbeta, cnt;  // cnt = detCntIdx + 1 - 0.5
+  BackEpi epi;
+  int zt0;
+};
+
+// The reference backprojector's formula (AAPM_script/MultiSlicesBackGPU.cu:
+// 115-184), geometry as in k_back_ref (FP64, once per voxel and view of the
+// tile); the difference of the two channel prefix-sum samples is walked over
+// the residual itself.
+template <int ZL>
+__global__ void __launch_bounds__(256, DDFAN_REF_MIN_CTAS) k_back_ref_dd(DdRefArgs a) {
+  using T = BackTile<ZL>;
+  constexpr int NT = T::NT, VG = T::VG, SPL = T::SPL, KT = T::KT, LT = T::LT, NV = T::NV;
+  constexpr int VC = (2048 / NV) < 1 ? 1 : ((2048 / NV) > 4 ? 4 : 2048 / NV);
+  __shared__ int2 s_i[VC][NV];
+  __shared__ float2 s_f[VC][NV];
+  __shared__ float s_w[VC][NV];
+  __shared__ int s_p[VC];
+  const int tid = threadIdx.x;
+  const int zl = tid % ZL, g = tid / ZL;
+  const int zt = blockIdx.z + a.zt0;
+  const int zb = zt * ZL + zl;
+  const int ntx = (a.XN + KT - 1) / KT;
+  const int ty = blockIdx.x / ntx, tx = blockIdx.x - ty * ntx;
+  const int y0 = ty * LT, x0 = tx * KT;
+  const int l = g / SPL, sg = g - l * SPL;
+  const int iy = y0 + l, ixs = x0 + sg * VG;
+  const bool active = zb < a.P4 && iy < a.YN && ixs < a.XN;
+  float acc[VG][4];
+#pragma unroll
+  for (int v = 0; v < VG; ++v) acc[v][0] = acc[v][1] = acc[v][2] = acc[v][3] = 0.f;
+  const double Ud = (double)a.U;
+  const size_t P4 = (size_t)a.P4;
+  const size_t vstride = (size_t)(a.U + 1) * P4;
+  for (int v0 = 0; v0 < a.PN; v0 += VC) {
+    const int nvc = min(VC, a.PN - v0);
+    if (tid < VC) s_p[tid] = v0 + tid;
+    for (int e = tid; e < VC * NV; e += NT) {
+      const int vv = e / NV, r = e - vv * NV;
+      const int ly = r / KT, lx = r - ly * KT;
+      const int yy = y0 + ly, xx = x0 + lx;
+      int2 ii = make_int2(0, 0);
+      float2 ff = make_float2(0.f, 0.f);
+      float w = 0.f;
+      if (vv < nvc && yy < a.YN && xx < a.XN &&
+          (!a.epi.mask || a.epi.mask[(size_t)yy * a.XN + xx] != 0)) {
+        const ViewGeom& G = a.vg[v0 + vv];
+        const double sx = G.sx, sy = G.sy;
+        const double ddx = (xx - a.ocx) * a.dx - sx, ddy = (yy - a.ocy) * a.dx - sy;
+        const double l2 = ddx * ddx + ddy * ddy;
+        const double ln = sqrt(l2);
+        const double alpha = asin((sy * ddx - sx * ddy) * a.inv_sid / ln);
+        const double ddv = fabs(sx) > fabs(sy) ? ddx : ddy;
+        const double da = ddv / l2 * a.dx * 0.5;
+        w = (float)(a.dx / ddv * ln);
+        const double cL = fmin(fmax((alpha - da) * a.inv_dbeta + a.cnt, 0.0), Ud);
+        const double cR = fmin(fmax((alpha + da) * a.inv_dbeta + a.cnt, 0.0), Ud);
+        ii = make_int2(min((int)cL, a.U - 1), min((int)cR, a.U - 1));
+        ff = make_float2((float)(cL - ii.x), (float)(cR - ii.y));
+      }
+      s_i[vv][r] = ii;
+      s_f[vv][r] = ff;
+      s_w[vv][r] = w;
+    }
+    __syncthreads();
+    if (active) {
+      for (int vv = 0; vv < nvc; ++vv) {
+        const float4* base = a.q + (size_t)s_p[vv] * vstride + zb;
+#pragma unroll
+        for (int v = 0; v < VG; ++v) {
+          const int r = l * KT + sg * VG + v;
+          const int2 ii = s_i[vv][r];
+          const float2 ff = s_f[vv][r];
+          const float3 w = walk_weights(ii.x, ff.x, ii.y, ff.y, s_w[vv][r]);
+          fma4(acc[v], w.x, __ldg(base + (size_t)ii.x * P4));
+          const int dn = ii.y - ii.x;
+          if (dn != 0) {
+            const int st = dn > 0 ? 1 : -1, n = dn > 0 ? dn : -dn;
+            for (int i = 1; i < n; ++i) fma4(acc[v], w.y, __ldg(base + (size_t)(ii.x + i * st) * P4));
+            fma4(acc[v], w.z, __ldg(base + (size_t)ii.y * P4));
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (!active) return;
+#pragma unroll
+  for (int v = 0; v < VG; ++v)
+    if (ixs + v < a.XN) back_store(a.epi, ixs + v, iy, zb, a.XN, a.Z, false, acc[v]);
+}
+
+// ============================================================ staging
+
+// dst[pix][z] = z < Z ? src[pix][z] * mask[pix] : 0 for z < Zp (mask null = 1):
+// the masked image with its slices padded to a multiple of 4.
+static __global__ void k_stage_image(const float* __restrict__ src, int Z, const uint8_t* __restrict__ mask,
+                                     float* __restrict__ dst, int Zp, size_t npix) {
+  const size_t n = npix * Zp;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t pix = i / Zp;
+    const int z = (int)(i - pix * Zp);
+    float v = 0.f;
+    if (z < Z) {
+      v = src[pix * Z + z];
+      if (mask && mask[pix] == 0) v = 0.f;
+    }
+    dst[i] = v;
+  }
+}
+
+// dst[p][u][z] = src[p][u][z] * wgt[p][u] for u < U, z < Z; zero on the
+// guard channel u = U and on padding slices (wgt null = 1).
+static __global__ void k_stage_sino(const float* __restrict__ src, int Z, const float* __restrict__ wgt, int U,
+                                    float* __restrict__ dst, int Zp, size_t PN) {
+  const size_t n = PN * (U + 1) * Zp;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = i / Zp;
+    const int z = (int)(i - r * Zp);
+    const size_t p = r / (U + 1);
+    const int u = (int)(r - p * (U + 1));
+    float v = 0.f;
+    if (u < U && z < Z) {
+      const size_t e = p * U + u;
+      v = src[e * Z + z];
+      if (wgt) v *= wgt[e];
+    }
+    dst[i] = v;
+  }
+}
+
+// The published image of a solver that keeps masked voxels at 0 internally:
+// out[pix][z] = mask ? x[pix][z] : x0[pix][z], clamped at 0 when the updates
+// clamp (every update leaves a masked voxel at its initial value).
+static __global__ void k_publish_masked(const float* __restrict__ x, int Zi, const float* __restrict__ x0,
+                                        int Z, const uint8_t* __restrict__ mask, int clamp0,
+                                        float* __restrict__ out, size_t npix) {
+  const size_t n = npix * Z;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t pix = i / Z;
+    const int z = (int)(i - pix * Z);
+    float v;
+    if (!mask || mask[pix] != 0) {
+      v = x[pix * Zi + z];
+    } else {
+      v = x0[i];
+      if (clamp0) v = fmaxf(v, 0.f);
+    }
+    out[i] = v;
+  }
+}
+
+}  // namespace ddfan

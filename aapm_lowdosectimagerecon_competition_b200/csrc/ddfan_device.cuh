@@ -25,6 +25,11 @@
 namespace ddfan {
 
 constexpr int SAT_FP32 = 0, SAT_HILO = 1, SAT_FP64 = 2;
+// no prefix-sum tables: footprint differences read the values directly (ddfan_dd_kernels.cuh)
+constexpr int SAT_DIRECT = 3;
+
+// the cell format that stands in for SAT_DIRECT where a path keeps tables
+__host__ __device__ inline int cell_mode(int mode) { return mode == SAT_DIRECT ? SAT_HILO : mode; }
 
 template <int M> struct CellInfo;
 template <> struct CellInfo<SAT_FP32> { static constexpr int F4 = 2; };

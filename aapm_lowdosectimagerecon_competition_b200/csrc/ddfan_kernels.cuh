@@ -246,6 +246,7 @@ __global__ void __launch_bounds__(512) k_sat(SatSrc s, float4* __restrict__ out,
 }  // namespace ddfan
 
 #include "ddfan_proj_kernels.cuh"
+#include "ddfan_dd_kernels.cuh"
 
 namespace ddfan {
 

@@ -32,6 +32,7 @@ struct PlanDesc {
 struct Plan {
   int device = 0;
   int XN = 0, YN = 0, U = 0, Z = 0, ZB = 0, PNmax = 0, mode = 0, ZL = 1;
+  int P4 = 0;  // 4-slice blocks of the direct mode's operands: ceil(Z / 4)
   double x0 = 0, y0 = 0, dx = 1, ocx = 0, ocy = 0, detCntIdx = 0;
   double inv_dbeta = 0, inv_sid = 0;  // REF backprojector
   double sh0x = 0, sh0y = -1;         // unit vector source -> rotation centre, angle 0
@@ -46,11 +47,13 @@ struct Plan {
   uint8_t* d_mask = nullptr;
   float* d_tb = nullptr;
   uint16_t* d_lut = nullptr;
-  float4 *d_satx = nullptr, *d_saty = nullptr, *d_satq = nullptr;  // prefix-sum tables
+  // prefix-sum tables; in the direct mode d_satq holds the staged sinogram
+  // operand [PNmax][U+1][4 P4] and there are no image tables
+  float4 *d_satx = nullptr, *d_saty = nullptr, *d_satq = nullptr;
   ViewGeom* d_vg = nullptr;
   double2* d_fc = nullptr;
   float* d_cvd = nullptr;
-  float* d_tmp = nullptr;   // one image of scratch (exact adjoint, pass 1)
+  float* d_tmp = nullptr;   // one image of scratch (exact adjoint, pass 1; the direct mode's staged image)
   float* d_angs = nullptr;  // PNmax angles (host-angle entry points)
   int* d_order = nullptr;   // PNmax views in dispatch order (x-major first)
   int* d_counts = nullptr;  // {x-major views, others}
@@ -75,6 +78,9 @@ void dev_free(void* p, cudaStream_t st);
 void mark_use(Plan& p, cudaStream_t st);
 // z-blocks per z-tile for a stack of ZB 4-slice blocks
 int pow2_zl(int ZB);
+// the z-tile width a plan uses: pow2_zl, narrowed by the DDFAN_ZL environment
+// variable (1, 2, 4 or 8), or exactly zl_force when that is one of those
+int plan_zl(int ZB, int zl_force);
 // DD3Boundaries (AAPM_script/utilities.cuh:268-287), float-rounded like the reference stores them
 void boundaries(int n, const float* c, std::vector<double>& out);
 void plan_free(Plan* p);
@@ -114,6 +120,35 @@ int launch_back(const Plan& p, int back_mode, const ViewGeom* vg, const double2*
                 const int* order, const int* counts, int PN, const BackEpi& epi, cudaStream_t st,
                 const int4* ztd = nullptr);
 int launch_view_order(const ViewGeom* vg, int PN, int* order, int* counts, cudaStream_t st);
+
+// ---- direct mode (no prefix-sum tables; ddfan_dd_kernels.cuh)
+// OS-SART residual fused into the forward projector's store: out = ((y - A x)
+// / rowsum where rowsum != 0, else A x) * wgt (wgt null = 1).
+struct DdResidual {
+  const float* y = nullptr;       // measured [views][U][ystride]
+  const int* yview = nullptr;     // slot -> measured view
+  const float* rowsum = nullptr;  // [slot][U]
+  const float* wgt = nullptr;     // [slot][U] or null
+  int ystride = 0;
+};
+// Forward projection of the masked image img [YN][XN][4 P4] into
+// out[slot][orow][ostride] (slices [zlo, zhi) written).
+int launch_fwd_dd(const Plan& p, const float* img, const ViewGeom* vg, const double2* fc, const float* cvd,
+                  const int* order, int PN, float* out, int orow, int ostride, int zlo, int zhi,
+                  const DdResidual* res, cudaStream_t st);
+// Backprojection of w [slot][U+1][4 P4] (guard channel U = 0; weighted by
+// 1/|dir.axis| for the exact adjoint) with the epilogue `epi`.
+int launch_back_dd(const Plan& p, int back_mode, const float* w, const ViewGeom* vg, const double2* fc,
+                   const int* order, const int* counts, int PN, const BackEpi& epi, cudaStream_t st);
+// dst[pix][z < Zp] = z < Z ? src[pix][z] * mask : 0
+int launch_stage_image(const float* src, int Z, const uint8_t* mask, float* dst, int Zp, size_t npix,
+                       cudaStream_t st);
+// dst[p][u <= U][z < Zp] = u < U && z < Z ? src[p][u][z] * wgt[p][u] : 0
+int launch_stage_sino(const float* src, int Z, const float* wgt, int U, float* dst, int Zp, size_t PN,
+                      cudaStream_t st);
+// out[pix][z] = mask ? x[pix][z] : (clamp0 ? max(x0, 0) : x0)
+int launch_publish_masked(const float* x, int Zi, const float* x0, int Z, const uint8_t* mask, int clamp0,
+                          float* out, size_t npix, cudaStream_t st);
 // k_view_order over nr ranges (desc[r] = {first row, count, order offset, -> x-major count})
 int launch_view_order_ranges(const ViewGeom* vg, int4* desc, int nr, int* order, cudaStream_t st);
 int proj_dev_shared(Plan& p, const float* d_angs, int stride, int PN, const float* d_vol,

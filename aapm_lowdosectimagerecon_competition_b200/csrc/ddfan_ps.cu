@@ -50,6 +50,7 @@ static void ps_scan_kind(int mode, const PsScanArgs& a, cudaStream_t st) {
 }
 
 int ps_scan(int mode, int kind, const PsScanArgs& a, cudaStream_t st) {
+  mode = cell_mode(mode);  // these tables keep hi/lo cells in the direct mode
   if (a.N < 1 || a.N > 1024 || a.Nw < a.N + a.pad)
     return set_err(DDFAN_ERR_UNSUPPORTED, "slice-major prefix sums: %d values in %d cells", a.N, a.Nw);
   if (a.nlines < 1) return DDFAN_OK;
@@ -60,6 +61,7 @@ int ps_scan(int mode, int kind, const PsScanArgs& a, cudaStream_t st) {
 }
 
 int ps_fwd(int mode, const PsFwdArgs& a, int cnt, int Z, cudaStream_t st) {
+  mode = cell_mode(mode);  // these tables keep hi/lo cells in the direct mode
   if (cnt < 1 || Z < 1) return DDFAN_OK;
   if (cnt > 65535 || Z > 65535) return set_err(DDFAN_ERR_UNSUPPORTED, "slice-major forward: %d views x %d slices", cnt, Z);
   dim3 grid((a.U + 247) / 248, cnt, Z);
@@ -73,6 +75,7 @@ int ps_fwd(int mode, const PsFwdArgs& a, int cnt, int Z, cudaStream_t st) {
 }
 
 int ps_back(int mode, const PsBackArgs& a, int Z, cudaStream_t st) {
+  mode = cell_mode(mode);  // these tables keep hi/lo cells in the direct mode
   if (Z < 1) return DDFAN_OK;
   if (Z > 65535) return set_err(DDFAN_ERR_UNSUPPORTED, "slice-major backprojection: %d slices", Z);
   if (a.U + 1 > 1024 || a.M > 4096) return set_err(DDFAN_ERR_UNSUPPORTED, "slice-major backprojection: %d channels", a.U);
@@ -87,6 +90,7 @@ int ps_back(int mode, const PsBackArgs& a, int Z, cudaStream_t st) {
 }
 
 int ps_back_ref(int mode, const PsBackArgs& a, int Z, cudaStream_t st) {
+  mode = cell_mode(mode);  // these tables keep hi/lo cells in the direct mode
   if (Z < 1) return DDFAN_OK;
   if (Z > 65535) return set_err(DDFAN_ERR_UNSUPPORTED, "slice-major backprojection: %d slices", Z);
   dim3 grid((a.XN + 63) / 64, (a.YN + 4 * kPsBackRows - 1) / (4 * kPsBackRows), Z);

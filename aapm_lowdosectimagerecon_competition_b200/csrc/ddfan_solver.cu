@@ -190,6 +190,15 @@ struct Solver {
   float* d_tabx = nullptr;   // image rows table [Z][YN][XN] cells
   float* d_taby = nullptr;   // image columns table [Z][XN][YN] cells
   float* d_sq = nullptr;     // weighted residual table [Z][cstride][U+1] cells
+  // Direct mode (no prefix-sum tables; one angle list for all slices): the
+  // image d_x [YN][XN][Zi] has its slices padded to a multiple of 4 (Zi) and
+  // its masked voxels kept at 0, so the projector reads it as it is; d_ax holds
+  // the residual [PNmax][U+1][Zi] with a zero guard channel.  A masked voxel's
+  // published value is its initial one (d_x0, the caller's layout), clamped
+  // at 0 by the updates when they clamp -- what the table path computes there.
+  bool direct = false;
+  float* d_x0 = nullptr;
+  long long iters_done = 0;
   cudaStream_t own = nullptr;
   cudaEvent_t last_use = nullptr;  // recorded after work enqueued on a caller's stream
   cudaGraph_t graph = nullptr;
@@ -213,7 +222,7 @@ static void solver_free(Solver* s) {
   if (s->graph) cudaGraphDestroy(s->graph);
   void* ptrs[] = {s->d_vg, s->d_fc, s->d_cvd, s->d_yview, s->d_order, s->d_counts, s->d_rows, s->d_cols,
                   s->d_y, s->d_x, s->d_xprev, s->d_ax, s->d_t, s->d_perm, s->d_inv, s->d_soff, s->d_ztd,
-                  s->d_xu, s->d_stage, s->d_pang, s->d_xt, s->d_tabx, s->d_taby, s->d_sq};
+                  s->d_xu, s->d_stage, s->d_pang, s->d_xt, s->d_tabx, s->d_taby, s->d_sq, s->d_x0};
   for (void* q : ptrs) dev_free(q, s->own);
   if (s->own) cudaStreamDestroy(s->own);
   if (s->last_use) cudaEventDestroy(s->last_use);
@@ -228,6 +237,14 @@ static int salloc(Solver& s, T** p, size_t n) {
   const int rc = dev_alloc((void**)p, std::max<size_t>(n, 1) * sizeof(T), s.own);
   if (!rc) s.bytes += std::max<size_t>(n, 1) * sizeof(T);
   return rc;
+}
+
+// The internal image and sinogram use another slice order or count than the
+// caller's (windowed solver; direct mode with slices padded to a multiple of 4).
+static bool remapped(const Solver& s) { return s.win || (s.direct && s.Zi != s.Z); }
+// The image callers read lives in d_xu (published after iterations), not d_x.
+static bool published_copy(const Solver& s) {
+  return s.win || s.ps || (s.direct && (s.Zi != s.Z || s.P->has_mask));
 }
 
 // Slice gathers between the caller's slice order and the internal one:
@@ -324,7 +341,27 @@ static int solver_iteration(Solver& s, cudaStream_t st) {
     if ((rc = ps_subset(s, k, st))) return rc;
     n += 7;
   }
-  for (int k = 0; k < s.nsub && !s.ps; ++k) {
+  for (int k = 0; k < s.nsub && s.direct; ++k) {
+    const int o = s.off[k], c = s.cnt[k];
+    BackEpi e{};
+    e.out = s.d_x; e.xin = s.d_x; e.colsum = s.d_cols + (size_t)k * s.XN * s.YN;
+    e.nonneg = s.nonneg; e.mask = p.has_mask ? p.d_mask : nullptr; e.zlo = 0; e.zhi = s.Zi;
+    const ViewGeom* vg = s.d_vg + o;
+    const double2* fc = s.d_fc + (size_t)o * (s.U + 1);
+    const float* cvd = s.d_cvd + (size_t)o * s.U;
+    // project the current image and store the residual (y - A x) / rowSum,
+    // weighted for the exact adjoint (AAPM_script/OSSART_AAPM.m:85-88)
+    DdResidual r;
+    r.y = s.d_y; r.yview = s.d_yview + o; r.rowsum = s.d_rows + (size_t)o * s.U; r.wgt = adj ? cvd : nullptr;
+    r.ystride = s.Zi;
+    if ((rc = launch_fwd_dd(p, s.d_x, vg, fc, cvd, s.d_order + o, c, s.d_ax, s.U + 1, s.Zi, 0, s.Zi, &r, st)))
+      return rc;
+    // backproject, divide by colSum, add, optional clamp (:91-97)
+    if ((rc = launch_back_dd(p, s.back_mode, s.d_ax, vg, fc, s.d_order + o, s.d_counts + 2 * k, c, e, st)))
+      return rc;
+    n += adj ? 3 : 2;
+  }
+  for (int k = 0; k < s.nsub && !s.ps && !s.direct; ++k) {
     const int o = s.off[k], c = s.cnt[k];
     BackEpi e{};
     e.out = s.d_x; e.xin = s.d_x; e.colsum = s.d_cols + (size_t)k * s.XN * s.YN;
@@ -373,7 +410,10 @@ static int solver_iteration(Solver& s, cudaStream_t st) {
 // solvers), after iterations.
 static int solver_publish(Solver& s, cudaStream_t st) {
   if (s.ps) return ps_transpose(s.d_x, s.d_xu, 1, s.Z, s.XN * s.YN, st);
-  if (!s.win) return DDFAN_OK;
+  if (s.direct && s.P->has_mask)
+    return launch_publish_masked(s.d_x, s.Zi, s.d_x0, s.Z, s.P->d_mask, s.nonneg && s.iters_done > 0 ? 1 : 0,
+                                 s.d_xu, (size_t)s.XN * s.YN, st);
+  if (!remapped(s)) return DDFAN_OK;
   return gather_slices(s.d_x, s.Zi, s.d_xu, s.Z, s.d_inv, (size_t)s.XN * s.YN, st);
 }
 
@@ -500,6 +540,7 @@ static int solver_weights_cells(Solver& s, const PlanDesc& d, const std::vector<
   d1.SLN = 1;
   d1.PNmax = PNmax;
   d1.zl_force = 0;
+  d1.sat_mode = cell_mode(d.sat_mode);
   PlanPtr P1;
   int rc = plan_create(&P1.p, d1);
   if (rc) return rc;
@@ -558,6 +599,7 @@ static int solver_weights(Solver& s, const PlanDesc& d, const std::vector<float>
   d1.SLN = 1;
   d1.PNmax = 1;
   d1.zl_force = 0;
+  d1.sat_mode = cell_mode(d.sat_mode);
   PlanPtr P1;
   int rc = plan_create(&P1.p, d1);
   if (rc) return rc;
@@ -691,8 +733,16 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
     s.ps = want_ps || (s.win && !want_win && win_cost > threshold);
     if (s.ps) s.win = false;
   }
+  // the direct mode serves one angle list for all slices; the per-slice
+  // paths keep hi/lo tables
+  s.direct = sat_mode == SAT_DIRECT && !s.win && !s.ps;
+  if (sat_mode == SAT_DIRECT && !s.direct) sat_mode = cell_mode(sat_mode);
   if (s.win) {
     s.Zi = W.Zi; s.nzt = W.nzt; s.Mc = W.Mc; s.perm = W.perm; s.maxcnt = W.maxcnt;
+  } else if (s.direct) {
+    s.Zi = (SLN + 3) / 4 * 4;
+    s.perm.assign(s.Zi, -1);
+    for (int z = 0; z < SLN; ++z) s.perm[z] = z;
   } else {
     s.Zi = SLN;
   }
@@ -718,9 +768,28 @@ static int solver_create(Solver** out, float x0, float y0, int DNU, const float*
       (rc = salloc(s, &s.d_counts, 2 * (size_t)numOfOS)) || (rc = salloc(s, &s.d_rows, P * DNU)) ||
       (rc = salloc(s, &s.d_cols, (size_t)numOfOS * XN * YN)) || (rc = salloc(s, &s.d_y, P * DNU * s.Zi)) ||
       (rc = salloc(s, &s.d_x, V)) || (rc = salloc(s, &s.d_xprev, V)) ||
-      (rc = salloc(s, &s.d_ax, (size_t)std::max(PNmax, 1) * DNU * s.Zi)) || (rc = salloc(s, &s.d_t, 1)))
+      (rc = salloc(s, &s.d_ax, (size_t)std::max(PNmax, 1) * (DNU + (s.direct ? 1 : 0)) * s.Zi)) ||
+      (rc = salloc(s, &s.d_t, 1)))
     return rc;
   cudaStream_t st = s.own;
+  if (s.direct) {
+    // the residual's guard channel stays 0; slice maps for padded slices; the
+    // initial image where masked voxels keep it
+    DDFAN_CK(cudaMemsetAsync(s.d_ax, 0, sizeof(float) * (size_t)std::max(PNmax, 1) * (DNU + 1) * s.Zi, st));
+    const size_t Vc = (size_t)XN * YN * SLN;
+    if (s.Zi != SLN) {
+      std::vector<int> inv(SLN);
+      for (int z = 0; z < SLN; ++z) inv[z] = z;
+      if ((rc = salloc(s, &s.d_perm, s.Zi)) || (rc = salloc(s, &s.d_inv, SLN)) ||
+          (rc = salloc(s, &s.d_stage, P * DNU * SLN)))
+        return rc;
+      DDFAN_CK(cudaMemcpyAsync(s.d_perm, s.perm.data(), sizeof(int) * s.Zi, cudaMemcpyHostToDevice, st));
+      DDFAN_CK(cudaMemcpyAsync(s.d_inv, inv.data(), sizeof(int) * SLN, cudaMemcpyHostToDevice, st));
+    }
+    if (s.P->has_mask && (rc = salloc(s, &s.d_x0, Vc))) return rc;
+    if (published_copy(s) && (rc = salloc(s, &s.d_xu, Vc))) return rc;
+    DDFAN_CK(cudaStreamSynchronize(st));
+  }
   DDFAN_CK(cudaMemcpyAsync(s.d_yview, yview.data(), sizeof(int) * P, cudaMemcpyHostToDevice, st));
   if (s.ps) {
     // angles of view k + m * numOfOS of every slice z, per subset k: row (k, z, m)
@@ -833,13 +902,23 @@ DDFAN_API size_t ddfan_ossart_estimate_bytes(int XN, int YN, int DNU, int SLN, i
                                              int sat_mode) {
   if (numOfOS < 1 || PNall < numOfOS) return 0;
   const size_t PNmax = (size_t)(PNall + numOfOS - 1) / numOfOS;
-  const size_t U = (size_t)DNU, P = (size_t)PNall, V = (size_t)XN * YN * SLN;
-  const size_t plan = ddfan_plan_estimate_bytes(XN, YN, DNU, SLN, (int)PNmax, sat_mode);
+  const bool direct = sat_mode == SAT_DIRECT;
+  // the direct mode pads slices to a multiple of 4 and keeps a guard channel
+  const size_t Zi = direct ? (size_t)(SLN + 3) / 4 * 4 : (size_t)SLN;
+  const size_t U = (size_t)DNU, P = (size_t)PNall, V = (size_t)XN * YN * Zi;
+  const size_t plan = ddfan_plan_estimate_bytes(XN, YN, DNU, (int)Zi, (int)PNmax, sat_mode);
   if (!plan) return 0;
-  const size_t own = P * sizeof(ViewGeom) + P * (U + 1) * sizeof(double2) + P * U * sizeof(float) +
-                     3 * P * sizeof(int) + 2 * (size_t)numOfOS * sizeof(int) + P * U * sizeof(float) +
-                     (size_t)numOfOS * XN * YN * sizeof(float) + P * U * SLN * sizeof(float) +
-                     2 * V * sizeof(float) + PNmax * U * SLN * sizeof(float) + sizeof(double);
+  size_t own = P * sizeof(ViewGeom) + P * (U + 1) * sizeof(double2) + P * U * sizeof(float) +
+               3 * P * sizeof(int) + 2 * (size_t)numOfOS * sizeof(int) + P * U * sizeof(float) +
+               (size_t)numOfOS * XN * YN * sizeof(float) + P * U * Zi * sizeof(float) +
+               2 * V * sizeof(float) + PNmax * (U + (direct ? 1 : 0)) * Zi * sizeof(float) + sizeof(double);
+  // direct mode: the initial image and the published copy (masked solves;
+  // padded slices), sinogram staging and slice maps (padded slices)
+  if (direct) {
+    own += 2 * (size_t)XN * YN * SLN * sizeof(float);
+    if (Zi != (size_t)SLN) own += P * U * SLN * sizeof(float) + (Zi + SLN) * sizeof(int);
+  }
+  sat_mode = cell_mode(sat_mode);  // the set-up's weight kernels keep tables
   // transient at creation: the one-slice weight plan and the slice-major
   // weight buffers (geometry, row sums, ones, tables) over nsub x PNmax rows
   const size_t R = (size_t)numOfOS * PNmax, CB = sat_mode == SAT_FP32 ? 8 : 16;
@@ -869,7 +948,7 @@ DDFAN_API int ddfan_ossart_set_sinogram(ddfan_ossart* h, const float* proj, int 
     }
     int rc = ps_transpose(src, s->d_y, 1, (long long)s->PNall * s->U, s->Z, st);
     if (rc) return rc;
-  } else if (!s->win) {
+  } else if (!remapped(*s)) {
     DDFAN_CK(cudaMemcpyAsync(s->d_y, proj, sizeof(float) * n,
                              is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
   } else {
@@ -897,6 +976,14 @@ DDFAN_API int ddfan_ossart_set_image(ddfan_ossart* h, const float* img, int is_d
                              is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
     int rc = ps_transpose(s->d_xu, s->d_x, 1, (long long)s->XN * s->YN, s->Z, st);
     if (rc) return rc;
+  } else if (s->direct && (s->P->has_mask || s->Zi != s->Z)) {
+    // masked and padded copy; the initial image kept where the mask is 0
+    float* src = s->P->has_mask ? s->d_x0 : s->d_xu;
+    DDFAN_CK(cudaMemcpyAsync(src, img, sizeof(float) * n,
+                             is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    int rc = launch_stage_image(src, s->Z, s->P->has_mask ? s->P->d_mask : nullptr, s->d_x, s->Zi,
+                                (size_t)s->XN * s->YN, st);
+    if (rc) return rc;
   } else if (!s->win) {
     DDFAN_CK(cudaMemcpyAsync(s->d_x, img, sizeof(float) * n,
                              is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
@@ -910,6 +997,12 @@ DDFAN_API int ddfan_ossart_set_image(ddfan_ossart* h, const float* img, int is_d
                            cudaMemcpyDeviceToDevice, st));
   static const double one = 1.0;
   DDFAN_CK(cudaMemcpyAsync(s->d_t, &one, sizeof(double), cudaMemcpyHostToDevice, st));
+  s->iters_done = 0;
+  // the image callers read is the initial one until an iteration runs
+  if (s->direct && published_copy(*s)) {
+    int rc = solver_publish(*s, st);
+    if (rc) return rc;
+  }
   // the pageable host sources above must be consumed before returning
   DDFAN_CK(cudaStreamSynchronize(st));
   return DDFAN_OK;
@@ -924,6 +1017,7 @@ DDFAN_API int ddfan_ossart_iterate(ddfan_ossart* h, int numOfIter, int use_graph
     for (int it = 0; it < numOfIter; ++it) {
       int rc = solver_iteration(*s, st);
       if (rc) return rc;
+      ++s->iters_done;
     }
     int rc = solver_publish(*s, st);
     if (rc) return rc;
@@ -943,7 +1037,10 @@ DDFAN_API int ddfan_ossart_iterate(ddfan_ossart* h, int numOfIter, int use_graph
     s->graph = gr;
     DDFAN_CK(cudaGraphInstantiate(&s->gexec, s->graph, 0));
   }
-  for (int it = 0; it < numOfIter; ++it) DDFAN_CK(cudaGraphLaunch(s->gexec, st));
+  for (int it = 0; it < numOfIter; ++it) {
+    DDFAN_CK(cudaGraphLaunch(s->gexec, st));
+    ++s->iters_done;
+  }
   int rc = solver_publish(*s, st);
   if (rc) return rc;
   cudaEventRecord(s->last_use, st);
@@ -956,7 +1053,7 @@ DDFAN_API int ddfan_ossart_get_image(ddfan_ossart* h, float* img, int is_device,
   DeviceGuard g(s->device);
   const size_t n = (size_t)s->XN * s->YN * s->Z;
   cudaStream_t st = (cudaStream_t)stream;
-  DDFAN_CK(cudaMemcpyAsync(img, (s->win || s->ps) ? s->d_xu : s->d_x, sizeof(float) * n,
+  DDFAN_CK(cudaMemcpyAsync(img, published_copy(*s) ? s->d_xu : s->d_x, sizeof(float) * n,
                            is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
   cudaEventRecord(s->last_use, st);
   if (!is_device) DDFAN_CK(cudaStreamSynchronize(st));
@@ -972,8 +1069,12 @@ DDFAN_API int ddfan_ossart_profile(ddfan_ossart* h, int numOfIter, void* stream,
   LaunchProfiler prof;
   active_profiler() = &prof;
   int rc = DDFAN_OK;
-  for (int it = 0; it < numOfIter && !rc; ++it) rc = solver_iteration(*s, st);
+  for (int it = 0; it < numOfIter && !rc; ++it) {
+    rc = solver_iteration(*s, st);
+    if (!rc) ++s->iters_done;
+  }
   active_profiler() = nullptr;
+  if (!rc) rc = solver_publish(*s, st);
   if (rc) return rc;
   DDFAN_CK(cudaStreamSynchronize(st));
   for (int k = 0; k < KIND_COUNT; ++k) {
@@ -991,13 +1092,15 @@ DDFAN_API int ddfan_ossart_profile(ddfan_ossart* h, int numOfIter, void* stream,
 
 DDFAN_API float* ddfan_ossart_image_ptr(ddfan_ossart* h) {
   Solver* s = reinterpret_cast<Solver*>(h);
-  return s ? ((s->win || s->ps) ? s->d_xu : s->d_x) : nullptr;
+  return s ? (published_copy(*s) ? s->d_xu : s->d_x) : nullptr;
 }
 
 DDFAN_API int ddfan_ossart_launches_per_iter(const ddfan_ossart* h) {
   const Solver* s = reinterpret_cast<const Solver*>(h);
   if (!s) return 0;
-  return s->nsub * (s->ps ? 7 : (s->back_mode == DDFAN_BACK_ADJ ? 5 : 4)) + (s->useFISTA ? 2 : 0);
+  const bool adj = s->back_mode == DDFAN_BACK_ADJ;
+  const int per = s->ps ? 7 : (s->direct ? (adj ? 3 : 2) : (adj ? 5 : 4));
+  return s->nsub * per + (s->useFISTA ? 2 : 0);
 }
 
 DDFAN_API int ddfan_OSSART_AAPM(float x0, float y0, int DNU, const float* xds, const float* yds,

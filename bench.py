@@ -39,13 +39,15 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--sat", default="hilo", choices=["fp32", "hilo", "fp64"])
+    ap.add_argument("--sat", default="hilo", choices=["fp32", "hilo", "fp64", "direct"])
     ap.add_argument("--back", default="adj", choices=["ref", "adj"])
     ap.add_argument("--slices", type=int, default=128)
     ap.add_argument("--subsets", type=int, default=24, help="c3: ordered subsets (the configuration has 24)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the final-image check against the FP64 oracle (and the CPU baseline it times)")
     ap.add_argument("--kernels", action="store_true",
                     help="time only one subset's projector kernels (small case for ncu captures)")
     ap.add_argument("--config", default="c3", choices=["c3", "c4", "c5", "rebin"],
@@ -634,6 +636,10 @@ def run_ours(args):
     # backprojection 4S + 4V (read the subset residual table once, write the image)
     alg = {"fwd": 4.0 * (V + S_sub), "back_a": 4.0 * (V + S_sub), "back_b": 4.0 * (V + S_sub),
            "sat_image": 4.0 * V + 2 * 12.0 * V, "sat_sino": 4.0 * S_sub + 12.0 * S_sub}
+    if args.sat == "direct":
+        # the forward also reads the measured sinogram and writes the residual
+        # (the prefix-sum kernels it replaces did that)
+        alg["fwd"] = 4.0 * V + 8.0 * S_sub
     top_ms = prof[top][0] / max(prof[top][1], 1)
     peak, peak_kind = peaks()
     achieved = alg[top] / (top_ms / 1e3) / 1e9
@@ -644,7 +650,7 @@ def run_ours(args):
                 "kernel_ms_per_iter": {k: round(v[0], 3) for k, v in prof.items()},
                 "note": "achieved = algorithmic bytes per launch / CUDA-event launch time; the "
                         "path is gather/issue bound, not HBM bound"}
-    if top == "fwd" and args.views == "shared":
+    if top == "fwd" and args.views == "shared" and args.sat != "direct":
         # the bound that applies: L1 gathers of prefix-sum cells -- per line of
         # each ray group one cell per boundary (CG channels share CG + 1
         # boundaries), a cell holding 4 slices (32 B FP32, 48 B hi/lo or FP64)
@@ -687,32 +693,76 @@ def run_ours(args):
         if world > 1:
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         te = float(tt.item())
+        h2d = int(y_h.numel() * 4 + x_h.numel() * 4 + s.PN * s.SLN * 4)
+        d2h = int(out_h.numel() * 4)
         line["e2e"] = {"value": world * e2e_iters / te, "unit": UNIT,
-                       "h2d_bytes_per_step": int(y_h.numel() * 4 + x_h.numel() * 4 +
-                                                 s.PN * s.SLN * 4),
-                       "d2h_bytes_per_step": int(out_h.numel() * 4),
-                       "step": "one ddfan_OSSART_AAPM call: solver set-up, weights, %d iterations, "
-                               "pinned H2D of sinogram+image, D2H of the image" % e2e_iters,
+                       "h2d_bytes_per_step": h2d // e2e_iters, "d2h_bytes_per_step": d2h // e2e_iters,
+                       "h2d_bytes_per_call": h2d, "d2h_bytes_per_call": d2h,
+                       "step": "one iteration of a ddfan_OSSART_AAPM call (solver set-up, weights, %d "
+                               "iterations, pinned H2D of sinogram+image, D2H of the image); bytes per step "
+                               "are the call's over its %d iterations" % (e2e_iters, e2e_iters),
                        "seconds_per_call": te}
 
     # ---- plain FP32 DD, one instance per launch, host round trips per subset
     if not args.no_plain and rank == 0:
         line["plain_fp32"] = plain_fp32_iteration(s, (x0, y0, xds, yds), y, mask)
 
-    if rank == 0 and world == 1 and not args.no_cpu:
-        sample = 2
-        sec, nt = cpu_port_timing(s, sample, 1)
-        line["cpu_baseline"] = {"value": 1.0 / (sec * s.SLN / sample), "unit": UNIT, "cores": nt,
-                                "kind": "port",
-                                "sample": "1 OS-SART iteration (24 subsets, 2304 views, FP64, ADJ) on "
-                                          "%d of %d slices, scaled by %d/%d" % (sample, s.SLN, s.SLN,
-                                                                               sample)}
+    # ---- final-image parity at this configuration, and the CPU baseline
+    parity_failed = False
+    if rank == 0 and not args.no_parity:
+        par, cpu = parity_check(s, (x0, y0, xds, yds), y, mask, hangs, solver, stream, args)
+        line["parity"] = par
+        parity_failed = not par["ok"]
+        if world == 1 and not args.no_cpu:
+            line["cpu_baseline"] = cpu
     solver.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+    if parity_failed:
+        print("PARITY FAILURE: final image rel-L2 %.3g above the bound %.0e against the FP64 oracle"
+              % (line["parity"]["rel_l2"], line["parity"]["bound"]), file=sys.stderr, flush=True)
+        sys.exit(3)
+
+
+PARITY_BOUND = 1e-5
+
+
+def parity_check(s, geom, y, mask, hangs, solver, stream, args):
+    """The workload's own final image against the FP64 oracle: the GPU solves
+    every slice for s.numOfIter iterations from zero; the oracle solves slices
+    0 and 77 of the same sinogram (slices are independent given the subset
+    weights, which both take from slice 0's angles, AAPM_script/
+    OSSART_AAPM.m:61-64).  The oracle's iteration time is the CPU baseline."""
+    import torch
+    from oracle import oracle as O
+    x0, y0, xds, yds = geom
+    iters = s.numOfIter
+    solver.set_image(torch.zeros((s.YN, s.XN, s.SLN), device=y.device))
+    solver.iterate(iters, use_graph=True, stream=stream)
+    torch.cuda.synchronize(y.device)
+    xg = solver.image().cpu().numpy().astype(np.float64)
+    pick = sorted({0, min(77, s.SLN - 1)})
+    ys = np.ascontiguousarray(y.cpu().numpy()[:, :, pick])
+    hs = np.ascontiguousarray(np.asarray(hangs)[:, pick])
+    init = np.zeros((s.YN, s.XN, len(pick)), np.float32)
+    nt = os.cpu_count() or 1
+    xo, secs = O.ossart(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0.0, 0.0, hs, s.PN, s.XN, s.YN, len(pick), ys, init,
+                        s.dx, mask, iters, s.numOfOS, s.useFISTA, s.nonneg,
+                        back_mode=O.ADJ if args.back == "adj" else O.REF, nthreads=nt, timing=True)
+    d = xg[:, :, pick] - xo
+    rel = float(np.linalg.norm(d.ravel()) / np.linalg.norm(xo.ravel()))
+    par = {"rel_l2": rel, "max_abs": float(np.abs(d).max()), "image_max": float(np.abs(xo).max()),
+           "slices": pick, "iterations": iters, "bound": PARITY_BOUND, "ok": rel <= PARITY_BOUND,
+           "against": "FP64 CPU oracle (oracle/ddfan_oracle.c), same sinogram, from zero"}
+    per_iter = secs / iters
+    cpu = {"value": 1.0 / (per_iter * s.SLN / len(pick)), "unit": UNIT, "cores": nt, "kind": "port",
+           "sample": "%d OS-SART iterations (%d subsets, %d views, FP64, %s) on slices %s of %d, per-iteration "
+                     "time scaled by %d/%d (slices are independent); the same run is the parity check"
+                     % (iters, s.numOfOS, s.PN, args.back.upper(), pick, s.SLN, s.SLN, len(pick))}
+    return par, cpu
 
 
 def _ossart_host(s, geom, y_h, x_h, out_h, mask, iters, args):

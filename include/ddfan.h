@@ -42,6 +42,11 @@ extern "C" {
 #define DDFAN_SAT_FP32 0 /* plain FP32 sums (the reference's precision class) */
 #define DDFAN_SAT_HILO 1 /* compensated hi/lo FP32 pairs */
 #define DDFAN_SAT_FP64 2 /* FP64 sums */
+/* no tables: each difference of two interpolated prefix sums is evaluated as
+ * the sum of the values it telescopes to (exact overlap weights, FP32, no
+ * cancellation).  Used on the paths with one angle list for all slices; paths
+ * that keep tables (per-slice angle lists) use hi/lo cells in this mode. */
+#define DDFAN_SAT_DIRECT 3
 
 /* backprojector */
 #define DDFAN_BACK_REF 0 /* the reference backprojector's formula (MultiSlicesBackGPU.cu:115-184) */
@@ -148,16 +153,21 @@ DDFAN_API int ddfan_back_dev(ddfan_plan* plan, const float* d_angs, int PN, int 
  * owned up front by another allocator (a framework's caching allocator, a pool
  * reserved at start-up), or they cannot take cudaMalloc's implicit device-wide
  * synchronisation mid-pipeline.  Same result as ddfan_proj_dev on a plan of the
- * same geometry; device inputs d_angs[PN] (one angle list for all slices) and
- * d_vol[YN][XN][SLN], device output d_prj[PN][DNU][SLN]; xds, yds and mask
- * (may be NULL) are host arrays.  Runs on the calling thread's current device.
- * All scratch (geometry and prefix-sum tables) lives in one fixed device array
- * of DDFAN_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds
- * until exit; a problem needing more returns DDFAN_ERR_UNSUPPORTED before any
- * GPU work.  The first call on a device looks up that array's device address
- * (cudaGetSymbolAddress): make it before capturing a stream.  Calls share the
- * array, so calls whose kernels overlap on one GPU race: serialise them (one
- * stream, or events). */
+ * same geometry and sat_mode (any of the four); device inputs d_angs[PN] (one
+ * angle list for all slices) and d_vol[YN][XN][SLN], device output
+ * d_prj[PN][DNU][SLN]; xds, yds and mask (may be NULL) are host arrays, read
+ * before the call returns.  Runs on the calling thread's current device.
+ * All scratch (geometry and prefix-sum tables, or the staged image of the
+ * direct mode) lives in one fixed device array of DDFAN_NOALLOC_SCRATCH_BYTES
+ * that every GPU loading this library holds until exit; a problem needing more
+ * returns DDFAN_ERR_UNSUPPORTED before any GPU work.  The first call on a device
+ * -- and the first after a cudaDeviceReset, which gives the device a new
+ * context -- looks up that array's device address (cudaGetSymbolAddress);
+ * make that first call before any stream capture.  A call made while its
+ * stream is being captured returns DDFAN_ERR_UNSUPPORTED: every call uploads
+ * its geometry from host memory that is gone when it returns.  Calls share
+ * the array, so calls whose kernels overlap on one GPU race: serialise them
+ * (one stream, or events). */
 #define DDFAN_NOALLOC_SCRATCH_BYTES (64ull << 20)
 DDFAN_API int ddfan_proj_noalloc(float x0, float y0, int DNU, const float* xds, const float* yds,
                                  float imgXCenter, float imgYCenter, const float* d_angs, int PN,

@@ -2,8 +2,10 @@
 with the reference's own kernels.  Needs a B200.
 
 Tolerances (relative L2 against the FP64 oracle):
-  compensated hi/lo or FP64 prefix sums: 2e-6 per projection/backprojection,
-  1e-5 on an OS-SART image; plain FP32 prefix sums: 5e-5 at these sizes.
+  compensated hi/lo or FP64 prefix sums, and the direct mode (footprint
+  differences summed from the values, no tables): 2e-6 per
+  projection/backprojection, 1e-5 on an OS-SART image; plain FP32 prefix sums:
+  5e-5 at these sizes.
 """
 import math
 import os
@@ -20,7 +22,8 @@ def rel(a, b):
     return float(np.linalg.norm((np.asarray(a, np.float64) - b).ravel()) / np.linalg.norm(np.ravel(b)))
 
 
-TOL = {"fp32": 5e-5, "hilo": 2e-6, "fp64": 2e-6}
+TOL = {"fp32": 5e-5, "hilo": 2e-6, "fp64": 2e-6, "direct": 2e-6}
+SATS = ["fp32", "hilo", "fp64", "direct"]
 
 
 @pytest.fixture(scope="module")
@@ -87,7 +90,7 @@ def obwd(O, g, prj, mode):
 
 
 @pytest.mark.parametrize("case", sorted(CASES))
-@pytest.mark.parametrize("sat", ["fp32", "hilo", "fp64"])
+@pytest.mark.parametrize("sat", SATS)
 def test_forward_matches_oracle(mods, case, sat):
     dd2, configs, device, O = mods
     g, vol, _ = make_case(configs, dd2, **CASES[case])
@@ -95,7 +98,7 @@ def test_forward_matches_oracle(mods, case, sat):
 
 
 @pytest.mark.parametrize("case", sorted(CASES))
-@pytest.mark.parametrize("sat", ["fp32", "hilo", "fp64"])
+@pytest.mark.parametrize("sat", SATS)
 @pytest.mark.parametrize("back", ["ref", "adj"])
 def test_backprojection_matches_oracle(mods, case, sat, back):
     dd2, configs, device, O = mods
@@ -107,7 +110,7 @@ def test_backprojection_matches_oracle(mods, case, sat, back):
         assert np.all(out[g["mask"] == 0] == 0)
 
 
-@pytest.mark.parametrize("sat", ["hilo", "fp64"])
+@pytest.mark.parametrize("sat", ["hilo", "fp64", "direct"])
 def test_adjoint_identity_on_gpu(mods, sat):
     dd2, configs, device, O = mods
     g, vol, prj = make_case(configs, dd2, XN=48, YN=40, SLN=8, PN=90, DNU=96, masked=True)
@@ -153,18 +156,19 @@ def test_start_idx_slabs_match_single_slab(mods):
         dd2.MultiSlicesProjGPU(*args, startIdx=[1, 4])
 
 
-def test_device_api_matches_host_api(mods):
+@pytest.mark.parametrize("sat", ["hilo", "direct"])
+def test_device_api_matches_host_api(mods, sat):
     import torch
     dd2, configs, device, O = mods
     g, vol, prj = make_case(configs, dd2, SLN=12)
     pl = device.Plan(g["x0"], g["y0"], g["DNU"], g["xds"], g["yds"], g["cnt"], g["XN"], g["YN"], g["SLN"],
-                     g["PN"], g["dx"], sat="hilo")
+                     g["PN"], g["dx"], sat=sat)
     angs = torch.from_numpy(np.ascontiguousarray(g["h"][:, 0])).cuda()
     p_dev = pl.proj(angs, torch.from_numpy(vol).cuda()).cpu().numpy()
-    np.testing.assert_allclose(p_dev, fwd(dd2, g, vol, "hilo"), rtol=1e-6, atol=1e-7)
+    np.testing.assert_allclose(p_dev, fwd(dd2, g, vol, sat), rtol=1e-6, atol=1e-7)
     for back in ("ref", "adj"):
         b_dev = pl.back(angs, torch.from_numpy(prj).cuda(), mode=back).cpu().numpy()
-        np.testing.assert_allclose(b_dev, bwd(dd2, g, prj, "hilo", back), rtol=1e-6, atol=1e-7)
+        np.testing.assert_allclose(b_dev, bwd(dd2, g, prj, sat, back), rtol=1e-6, atol=1e-7)
     # per-slice angle tensor (PN, SLN) takes the grouped path
     hp = torch.from_numpy(np.ascontiguousarray(g["h"])).cuda()
     np.testing.assert_allclose(pl.proj(hp, torch.from_numpy(vol).cuda()).cpu().numpy(), p_dev,
@@ -183,21 +187,43 @@ def solver_case(configs, dd2, O, SLN=6, XN=40, PN=96, DNU=64, nsub=6):
     return s, (x0, y0, xds, yds), xt, mask, y
 
 
+@pytest.mark.parametrize("sat", ["hilo", "direct"])
 @pytest.mark.parametrize("back", ["ref", "adj"])
 @pytest.mark.parametrize("nonneg", [0, 1])
-def test_ossart_matches_oracle(mods, back, nonneg):
+def test_ossart_matches_oracle(mods, back, nonneg, sat):
     dd2, configs, device, O = mods
     s, (x0, y0, xds, yds), xt, mask, y = solver_case(configs, dd2, O)
     init = np.zeros_like(xt)
-    xg = dd2.OSSART_AAPM(y, s.hangs(), init, s.conf(), 5, s.numOfOS, mask, 1, nonneg, sat="hilo", back=back)
+    xg = dd2.OSSART_AAPM(y, s.hangs(), init, s.conf(), 5, s.numOfOS, mask, 1, nonneg, sat=sat, back=back)
     xo = O.ossart(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0, 0, s.hangs(), s.PN, s.XN, s.YN, s.SLN, y, init,
                   s.dx, mask, 5, s.numOfOS, 1, nonneg, O.REF if back == "ref" else O.ADJ)
     assert rel(xg, xo) < 1e-5
     if nonneg:
         # the clamp follows every subset update; FISTA's extrapolation after the
         # last subset may dip below 0, so check the clamp without momentum
-        x1 = dd2.OSSART_AAPM(y, s.hangs(), init, s.conf(), 2, s.numOfOS, mask, 0, 1, sat="hilo", back=back)
+        x1 = dd2.OSSART_AAPM(y, s.hangs(), init, s.conf(), 2, s.numOfOS, mask, 0, 1, sat=sat, back=back)
         assert x1.min() >= 0
+
+
+@pytest.mark.parametrize("back", ["ref", "adj"])
+@pytest.mark.parametrize("SLN", [5, 8])
+def test_direct_solver_masked_initial_image(mods, back, SLN):
+    """The direct mode keeps masked voxels at 0 inside the solver and pads the
+    slices to a multiple of 4; the image it returns must still be the table
+    path's: masked voxels keep their initial value (clamped at 0 by the
+    non-negativity step), and FISTA momentum leaves them there."""
+    dd2, configs, device, O = mods
+    s, (x0, y0, xds, yds), xt, mask, y = solver_case(configs, dd2, O, SLN=SLN)
+    rng = np.random.default_rng(11)
+    init = (rng.random(xt.shape) * 0.02 - 0.005).astype(np.float32)
+    xg = dd2.OSSART_AAPM(y, s.hangs(), init, s.conf(), 3, s.numOfOS, mask, 1, 1, sat="direct", back=back)
+    xo = O.ossart(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0, 0, s.hangs(), s.PN, s.XN, s.YN, s.SLN, y, init,
+                  s.dx, mask, 3, s.numOfOS, 1, 1, O.REF if back == "ref" else O.ADJ)
+    assert rel(xg, xo) < 1e-5
+    m0 = mask == 0
+    np.testing.assert_array_equal(xg[m0], np.maximum(init[m0], 0))
+    xh = dd2.OSSART_AAPM(y, s.hangs(), init, s.conf(), 3, s.numOfOS, mask, 1, 1, sat="hilo", back=back)
+    assert rel(xg, xh) < 1e-5
 
 
 def rebinned_angles(PN, SLN, starts, BV=0.3):
@@ -258,14 +284,15 @@ def test_ossart_per_slice_angles_matches_oracle(mods, monkeypatch, back, path, l
     assert rel(xg[:, :, :1], x_first) < 1e-6
 
 
-def test_ossart_graph_equals_stream_launches(mods):
+@pytest.mark.parametrize("sat", ["hilo", "direct"])
+def test_ossart_graph_equals_stream_launches(mods, sat):
     import torch
     dd2, configs, device, O = mods
     s, (x0, y0, xds, yds), xt, mask, y = solver_case(configs, dd2, O, SLN=8)
     res = []
     for graph in (True, False):
         sv = device.OSSART(x0, y0, s.DNU, xds, yds, s.detCntIdx, s.hangs(), s.XN, s.YN, s.SLN, s.dx, mask=mask,
-                           numOfOS=s.numOfOS, useFISTA=1, nonneg=1, sat="hilo", back="adj")
+                           numOfOS=s.numOfOS, useFISTA=1, nonneg=1, sat=sat, back="adj")
         sv.set_sinogram(torch.from_numpy(y).cuda())
         sv.set_image(torch.zeros((s.YN, s.XN, s.SLN)).cuda())
         sv.iterate(3, use_graph=graph)
@@ -286,11 +313,11 @@ def test_compensated_sums_beat_fp32_at_full_width(mods):
     vol = configs.ellipsoid_phantom_3d(s)
     exp = O.proj(x0, y0, s.DNU, xds, yds, 0, 0, h, PN, s.XN, s.YN, s.SLN, vol, s.dx)
     err = {}
-    for sat in ("fp32", "hilo", "fp64"):
+    for sat in ("fp32", "hilo", "fp64", "direct"):
         got = dd2.MultiSlicesProjGPU(x0, y0, s.DNU, xds, yds, 0, 0, h, PN, s.XN, s.YN, s.SLN, vol, s.dx,
                                      sat=sat)
         err[sat] = rel(got, exp)
-    assert err["hilo"] < 1e-6 and err["fp64"] < 1e-6
+    assert err["hilo"] < 1e-6 and err["fp64"] < 1e-6 and err["direct"] < 1e-6
     assert err["fp32"] > err["hilo"]
 
 
