@@ -9,6 +9,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -620,16 +621,36 @@ int launch_publish_masked(const float* x, int Zi, const float* x0, int Z, const 
   return check_launch("k_publish_masked");
 }
 
+// channels per thread of the direct forward projector for a z-lane count
+#ifndef DDFAN_DD_FWD_CG
+#define DDFAN_DD_FWD_CG 1
+#endif
+template <int ZL> struct DdFwdCG { static constexpr int v = ZL >= 4 ? DDFAN_DD_FWD_CG : (ZL == 2 ? 2 : 1); };
+
+// z-tiles per thread of the direct kernels: each decoded footprint serves
+// 4 slices per z-tile, so more z-tiles per thread means fewer instructions
+// per slice (the measured lever: 1 -> 4 took a 96-view c3 subset's forward
+// from 3.5 to 2.6 ms); at most the call's z-tiles
+static int dd_nz(int nzt) { return nzt >= 4 && DDFAN_DD_NZ >= 4 ? 4 : (nzt >= 2 && DDFAN_DD_NZ >= 2 ? 2 : 1); }
+
 template <int ZL>
 static void fwd_dd_go(const DdFwdArgs& a, int nzt, cudaStream_t st) {
-  constexpr int CG = FwdCG<ZL>::v;
-  using T = DdFwdTile<ZL, CG>;
+  constexpr int CG = DdFwdCG<ZL>::v;
   constexpr int kMaxRows = 65535;  // grid y limit
-  for (int r0 = 0; r0 < a.PN; r0 += kMaxRows) {
-    DdFwdArgs b = a;
-    b.row0 = r0;
-    dim3 grid((a.U + T::CW - 1) / T::CW, std::min(a.PN - r0, kMaxRows), nzt);
-    k_fwd_dd<ZL, CG><<<grid, T::NT, 0, st>>>(b);
+  const auto go = [&](auto nz) {
+    constexpr int NZ = decltype(nz)::value;
+    using T = DdFwdTile<ZL, CG, NZ>;
+    for (int r0 = 0; r0 < a.PN; r0 += kMaxRows) {
+      DdFwdArgs b = a;
+      b.row0 = r0;
+      dim3 grid((a.U + T::CW - 1) / T::CW, std::min(a.PN - r0, kMaxRows), (nzt + NZ - 1) / NZ);
+      k_fwd_dd<ZL, CG, NZ><<<grid, T::NT, 0, st>>>(b);
+    }
+  };
+  switch (dd_nz(nzt)) {
+    case 4: go(std::integral_constant<int, 4>()); break;
+    case 2: go(std::integral_constant<int, 2>()); break;
+    default: go(std::integral_constant<int, 1>()); break;
   }
 }
 
@@ -647,6 +668,7 @@ int launch_fwd_dd(const Plan& p, const float* img, const ViewGeom* vg, const dou
   }
   int nzt = 0;
   ztile_range(p, zlo, zhi, &a.zt0, &nzt);
+  a.nzt = nzt;
   if (nzt == 0 || PN < 1) return DDFAN_OK;
   ProfScope ps(KIND_FWD, st);
   switch (p.ZL) {
@@ -660,10 +682,14 @@ int launch_fwd_dd(const Plan& p, const float* img, const ViewGeom* vg, const dou
 
 template <int ZL, bool XM>
 static void back_dd_go(const DdAdjArgs& a, int nzt, cudaStream_t st) {
-  using T = BackTile<ZL>;
+  using T = DdBackTile<ZL>;
   const int nl = XM ? a.XN : a.YN, N = XM ? a.YN : a.XN;
   const int tiles = ((nl + T::LT - 1) / T::LT) * ((N + T::KT - 1) / T::KT);
-  k_back_dd<ZL, XM><<<dim3(tiles, 1, nzt), T::NT, 0, st>>>(a);
+  switch (dd_nz(nzt)) {
+    case 4: k_back_dd<ZL, XM, 4><<<dim3(tiles, 1, (nzt + 3) / 4), T::NT, 0, st>>>(a); break;
+    case 2: k_back_dd<ZL, XM, 2><<<dim3(tiles, 1, (nzt + 1) / 2), T::NT, 0, st>>>(a); break;
+    default: k_back_dd<ZL, XM, 1><<<dim3(tiles, 1, nzt), T::NT, 0, st>>>(a); break;
+  }
 }
 
 template <bool XM>
@@ -717,6 +743,7 @@ int launch_back_dd(const Plan& p, int back_mode, const float* w, const ViewGeom*
   a.PN = PN; a.U = p.U; a.Z = p.Z; a.XN = p.XN; a.YN = p.YN;
   a.ocx = p.ocx; a.ocy = p.ocy; a.dx = p.dx;
   a.zt0 = zt0;
+  a.nzt = nzt;
   // pass 1: x-major views along x columns -> tmp (mask applied)
   a.epi = epi;
   a.epi.out = p.d_tmp; a.epi.addend = nullptr; a.epi.xin = nullptr; a.epi.colsum = nullptr;

@@ -28,11 +28,14 @@
 
 namespace ddfan {
 
+// Resident CTAs per SM the register allocation is sized for (256 threads:
+// 2 -> up to 128 registers, which the 4-z-tile accumulators need without
+// spilling).  Build-time knobs for tuning sweeps, like the tile shapes below.
 #ifndef DDFAN_DD_FWD_MIN_CTAS
-#define DDFAN_DD_FWD_MIN_CTAS 3
+#define DDFAN_DD_FWD_MIN_CTAS 2
 #endif
 #ifndef DDFAN_DD_BACK_MIN_CTAS
-#define DDFAN_DD_BACK_MIN_CTAS 4
+#define DDFAN_DD_BACK_MIN_CTAS 2
 #endif
 
 __device__ __forceinline__ void fma4(float (&a)[4], float w, const float4& v) {
@@ -42,12 +45,64 @@ __device__ __forceinline__ void fma4(float (&a)[4], float w, const float4& v) {
   a[3] = fmaf(w, v.w, a[3]);
 }
 
-// Weights of the telescoped difference from (k0, f0) to (k1, f1), scaled by
-// `s`: value = w0 v[k0] + wi sum(interior) + we v[k1].
-__device__ __forceinline__ float3 walk_weights(int k0, float f0, int k1, float f1, float s) {
-  if (k1 == k0) return make_float3((f1 - f0) * s, 0.f, 0.f);
-  if (k1 > k0) return make_float3((1.f - f0) * s, s, f1 * s);
-  return make_float3(-f0 * s, -s, (f1 - 1.f) * s);
+// The walk from (k0, f0) to (k1, f1) as three weights: w0 on the value at
+// k0, wm on the value one step on (an interior value when n = |k1 - k0| >= 2,
+// else 0: that value is then the end value or past it), we on the value at k1
+// (0 when n = 0: it is the start value again); interior values beyond the
+// first (n > 2) take wm as well.  Scaled by s.
+__device__ __forceinline__ float3 walk3(int k0, float f0, int k1, float f1, float s) {
+  const int n = k1 > k0 ? k1 - k0 : k0 - k1;
+  if (n == 0) return make_float3((f1 - f0) * s, 0.f, 0.f);
+  const float wi = k1 > k0 ? s : -s;
+  return k1 > k0 ? make_float3((1.f - f0) * s, n >= 2 ? wi : 0.f, f1 * s)
+                 : make_float3(-f0 * s, n >= 2 ? wi : 0.f, (f1 - 1.f) * s);
+}
+
+// k0 and k1 of a walk packed in one word (indices below 32768)
+__device__ __forceinline__ int pack_k(int k0, int k1) { return k0 | (k1 << 16); }
+
+// Predicated 16-byte load through the read-only path into v, which keeps its
+// value when p is false (no memory access then).  One instruction, so the
+// loads of a walk issue back to back instead of behind branches; the kept
+// value is finite image or sinogram data, and every caller gives it weight 0.
+__device__ __forceinline__ void ldg4_keep(bool p, const float4* a, float4& v) {
+  asm("{\n\t.reg .pred q;\n\t"
+      "setp.ne.b32 q, %4, 0;\n\t"
+      "@q ld.global.nc.v4.f32 {%0, %1, %2, %3}, [%5];\n\t}"
+      : "+f"(v.x), "+f"(v.y), "+f"(v.z), "+f"(v.w)
+      : "r"((int)p), "l"(a));
+}
+
+// One walk for NZ z-tiles (float4 runs zoff[z] float4 past base): adds w0 cur
+// + wm v[k0 + st] + we v[k1] (+ wm v for the further interior values) to acc
+// and leaves v[k1] in cur.  v[k1] is loaded only when the walk moves (n >= 1;
+// else it is cur), the first interior value only when there is one (n >= 2,
+// into vm, which otherwise keeps an earlier value under weight 0): about two
+// loads per footprint, and no branch unless it spans more than two steps.
+template <int NZ>
+__device__ __forceinline__ void walk_nz(float (&acc)[NZ][4], float4 (&cur)[NZ], float4 (&vm)[NZ],
+                                        const float4* base, size_t stride, const int (&zoff)[NZ], int k0, int k1,
+                                        int kmax, const float4& wt) {
+  const int dn = k1 - k0, st = dn > 0 ? 1 : -1, n = dn > 0 ? dn : -dn;
+  const int km = min(max(k0 + st, 0), kmax);
+  const float4* pm = base + (size_t)km * stride;
+  const float4* pe = base + (size_t)k1 * stride;
+#pragma unroll
+  for (int z = 0; z < NZ; ++z) ldg4_keep(n >= 2, pm + zoff[z], vm[z]);
+#pragma unroll
+  for (int z = 0; z < NZ; ++z) fma4(acc[z], wt.x, cur[z]);
+#pragma unroll
+  for (int z = 0; z < NZ; ++z) ldg4_keep(n >= 1, pe + zoff[z], cur[z]);
+#pragma unroll
+  for (int z = 0; z < NZ; ++z) {
+    fma4(acc[z], wt.y, vm[z]);
+    fma4(acc[z], wt.z, cur[z]);
+  }
+  for (int i = 2; i < n; ++i) {
+    const float4* pi = base + (size_t)(k0 + i * st) * stride;
+#pragma unroll
+    for (int z = 0; z < NZ; ++z) fma4(acc[z], wt.y, __ldg(pi + zoff[z]));
+  }
 }
 
 // ============================================================ forward projector
@@ -63,7 +118,7 @@ struct DdFwdArgs {
   int orow, ostride;
   int PN, U, Z, XN, YN;
   float dx;
-  int zlo, zhi, zt0, row0;
+  int zlo, zhi, zt0, nzt, row0;
   // fused OS-SART residual (AAPM_script/OSSART_AAPM.m:86-88); y null = plain projection
   const float* y;      // measured [views][U][ystride]
   const int* yview;    // slot -> measured view
@@ -72,100 +127,130 @@ struct DdFwdArgs {
   int ystride;
 };
 
-template <int ZL, int CG>
+// Lines of a forward chunk unrolled together, geometry elements (line,
+// channel) a warp prepares per chunk, and z-tiles per thread.
+#ifndef DDFAN_DD_FWD_UNROLL
+#define DDFAN_DD_FWD_UNROLL 1
+#endif
+#ifndef DDFAN_DD_FWD_GEOM
+#define DDFAN_DD_FWD_GEOM 256
+#endif
+// most z-tiles per thread (1, 2 or 4; fewer when a call has fewer)
+#ifndef DDFAN_DD_NZ
+#define DDFAN_DD_NZ 4
+#endif
+
+template <int ZL, int CG, int NZ>
 struct DdFwdTile {
-  static constexpr int NT = 256;
-  static constexpr int NG = NT / ZL;     // channel groups
-  static constexpr int CW = NG * CG;     // channels per CTA
-  static constexpr int NB = CW + 1;
-  static constexpr int CC = 2048 / CW;   // lines per geometry chunk
+  static constexpr int NT = 256, NW = NT / 32;
+  static constexpr int GW = 32 / ZL;                  // channel groups per warp
+  static constexpr int CWW = GW * CG;                 // channels per warp
+  static constexpr int CW = NW * CWW;                 // channels per CTA
+  static constexpr int CC = DDFAN_DD_FWD_GEOM / CWW;  // lines per geometry chunk
+  static constexpr int UNROLL = DDFAN_DD_FWD_UNROLL;
 };
 
-// CTA = one view x CW channels x 4*ZL slices; a thread owns CG consecutive
-// channels x 4 slices and walks their footprints along each line, carrying
-// the value at the boundary two channels share.  Phase G (per chunk of CC
-// lines): for each channel the cell index of its first boundary and the walk
-// weights over 1 / footprint length (MultiSlicesProjGPU.cu:166-170).
-template <int ZL, int CG>
+// CTA = one view x CW channels x NZ z-tiles of 4*ZL slices; a thread owns CG
+// consecutive channels x 4 slices in each of its NZ z-tiles and walks their
+// footprints along each line, carrying the value at the boundary two channels
+// share.  Every warp prepares the geometry of its own CWW channels (per chunk
+// of CC lines: each channel's two cell indices and walk weights over
+// 1 / footprint length, MultiSlicesProjGPU.cu:166-170) and synchronises with
+// itself only, so warps interleave FP64 geometry with other warps' gathers.
+template <int ZL, int CG, int NZ>
 __global__ void __launch_bounds__(256, DDFAN_DD_FWD_MIN_CTAS) k_fwd_dd(DdFwdArgs a) {
-  using T = DdFwdTile<ZL, CG>;
-  constexpr int NT = T::NT, CW = T::CW, NB = T::NB, CC = T::CC;
-  __shared__ double2 s_fc[NB];
-  __shared__ int s_k[CC][CW];
-  __shared__ float4 s_w[CC][CW];  // (w0, wi, we) / length, step count as int bits
-  const int tid = threadIdx.x;
-  const int zl = tid % ZL, g = tid / ZL;
-  const int zt = blockIdx.z + a.zt0;
+  using T = DdFwdTile<ZL, CG, NZ>;
+  constexpr int NW = T::NW, CWW = T::CWW, CW = T::CW, CC = T::CC;
+  __shared__ double2 s_fc[NW][CWW + 1];
+  __shared__ float4 s_w[NW][CC][CWW];  // (w0, wm, we) / length; k0 | k1 << 16 as int bits
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  const int zl = lane % ZL, gw = lane / ZL;
   const int row = a.row0 + (int)blockIdx.y;
   if (row >= a.PN) return;  // uniform per CTA
   const int slot = a.order ? a.order[row] : row;
   const int p = slot;
-  const int zb = zt * ZL + zl;
-  const int ub0 = blockIdx.x * CW;
+  const int wc0 = blockIdx.x * CW + w * CWW;  // the warp's first channel
+  if (wc0 >= a.U) return;  // uniform per warp; no CTA-wide barrier follows
+  // z-tiles zt0 + blockIdx.z * NZ + z of the call's nzt; block zb = zt * ZL + zl
+  const int zt_first = a.zt0 + (int)blockIdx.z * NZ;
+  int zbk[NZ], zoff[NZ];
+  bool zok[NZ];
+#pragma unroll
+  for (int z = 0; z < NZ; ++z) {
+    zbk[z] = (zt_first + z) * ZL + zl;
+    zok[z] = (int)blockIdx.z * NZ + z < a.nzt && zbk[z] < a.P4;
+    zoff[z] = zok[z] ? z * ZL : 0;  // a tile past the image reads the first one again (dropped)
+  }
   const bool xm = a.vg[p].xmajor != 0;
   const int nl = xm ? a.XN : a.YN, N = xm ? a.YN : a.XN;
-  for (int b = tid; b < NB; b += NT) s_fc[b] = a.fc[(size_t)p * (a.U + 1) + min(ub0 + b, a.U)];
-  const bool active = (ub0 + g * CG < a.U) && (zb < a.P4);
+  for (int b = lane; b <= CWW; b += 32) s_fc[w][b] = a.fc[(size_t)p * (a.U + 1) + min(wc0 + b, a.U)];
+  const bool active = (wc0 + gw * CG < a.U) && zok[0];
   // x-major views integrate along x columns (line = x, k = y), the others along y rows
   const size_t P4 = (size_t)a.P4;
   const size_t kstride = (xm ? (size_t)a.XN : 1) * P4;
   const size_t lstride = (xm ? 1 : (size_t)a.XN) * P4;
-  const float4* img = a.img + (active ? zb : 0);
-  float acc[CG][4];
+  const float4* img = a.img + (active ? zbk[0] : 0);
+  float acc[CG][NZ][4];
+  float4 vm[NZ];  // first interior values (kept between walks; see walk_nz)
 #pragma unroll
-  for (int j = 0; j < CG; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+  for (int z = 0; z < NZ; ++z) vm[z] = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+  for (int j = 0; j < CG; ++j)
+#pragma unroll
+    for (int z = 0; z < NZ; ++z) acc[j][z][0] = acc[j][z][1] = acc[j][z][2] = acc[j][z][3] = 0.f;
   const double Nd = (double)N;
   const float dx = a.dx;
-  __syncthreads();
+  __syncwarp();
   for (int ii0 = 0; ii0 < nl; ii0 += CC) {
-    for (int e = tid; e < CC * CW; e += NT) {
-      const int col = e / CW, j = e - col * CW;
+    for (int e = lane; e < CC * CWW; e += 32) {
+      const int col = e / CWW, j = e - col * CWW;
       const double di = (double)(ii0 + col);
-      const double2 fa = s_fc[j], fb = s_fc[j + 1];
+      const double2 fa = s_fc[w][j], fb = s_fc[w][j + 1];
       const double c0 = fma(di, fa.x, fa.y), c1 = fma(di, fb.x, fb.y);
       const double cc0 = fmin(fmax(c0, 0.0), Nd), cc1 = fmin(fmax(c1, 0.0), Nd);
       const int k0 = min((int)cc0, N - 1), k1 = min((int)cc1, N - 1);
       const float f0 = (float)(cc0 - (double)k0), f1 = (float)(cc1 - (double)k1);
-      const float inv = ub0 + j < a.U ? __frcp_rn((float)(c1 - c0) * dx) : 0.f;
-      const float3 w = walk_weights(k0, f0, k1, f1, inv);
-      s_k[col][j] = k0;
-      s_w[col][j] = make_float4(w.x, w.y, w.z, __int_as_float(k1 - k0));
+      const float inv = wc0 + j < a.U ? __frcp_rn((float)(c1 - c0) * dx) : 0.f;
+      const float3 wt = walk3(k0, f0, k1, f1, inv);
+      s_w[w][col][j] = make_float4(wt.x, wt.y, wt.z, __int_as_float(pack_k(k0, k1)));
     }
-    __syncthreads();
+    __syncwarp();
     if (active) {
       const int ncol = min(CC, nl - ii0);
-      float part[CG][4];
+      float part[CG][NZ][4];
 #pragma unroll
-      for (int j = 0; j < CG; ++j) part[j][0] = part[j][1] = part[j][2] = part[j][3] = 0.f;
+      for (int j = 0; j < CG; ++j)
+#pragma unroll
+        for (int z = 0; z < NZ; ++z) part[j][z][0] = part[j][z][1] = part[j][z][2] = part[j][z][3] = 0.f;
+#pragma unroll(T::UNROLL)
       for (int col = 0; col < ncol; ++col) {
         const float4* line = img + (size_t)(ii0 + col) * lstride;
-        int k = s_k[col][g * CG];
-        float4 cur = __ldg(line + (size_t)k * kstride);
+        float4 cur[NZ];
+        {
+          const float4* p0 = line + (size_t)(__float_as_int(s_w[w][col][gw * CG].w) & 0xffff) * kstride;
+#pragma unroll
+          for (int z = 0; z < NZ; ++z) cur[z] = __ldg(p0 + zoff[z]);
+        }
 #pragma unroll
         for (int j = 0; j < CG; ++j) {
-          const float4 w = s_w[col][g * CG + j];
-          const int dn = __float_as_int(w.w);
-          fma4(part[j], w.x, cur);
-          if (dn != 0) {
-            const int st = dn > 0 ? 1 : -1, n = dn > 0 ? dn : -dn;
-            for (int i = 1; i < n; ++i) fma4(part[j], w.y, __ldg(line + (size_t)(k + i * st) * kstride));
-            k += dn;
-            cur = __ldg(line + (size_t)k * kstride);
-            fma4(part[j], w.z, cur);
-          }
+          const float4 wt = s_w[w][col][gw * CG + j];
+          const int pk = __float_as_int(wt.w);
+          walk_nz<NZ>(part[j], cur, vm, line, kstride, zoff, pk & 0xffff, pk >> 16, N - 1, wt);
         }
       }
 #pragma unroll
       for (int j = 0; j < CG; ++j)
 #pragma unroll
-        for (int s = 0; s < 4; ++s) acc[j][s] += part[j][s];
+        for (int z = 0; z < NZ; ++z)
+#pragma unroll
+          for (int s = 0; s < 4; ++s) acc[j][z][s] += part[j][z][s];
     }
-    __syncthreads();
+    __syncwarp();
   }
   if (!active) return;
 #pragma unroll
   for (int j = 0; j < CG; ++j) {
-    const int u = ub0 + g * CG + j;
+    const int u = wc0 + gw * CG + j;
     if (u >= a.U) break;
     const size_t e = (size_t)slot * a.U + u;
     const float cv = __ldg(a.cvd + e) * dx;
@@ -178,16 +263,20 @@ __global__ void __launch_bounds__(256, DDFAN_DD_FWD_MIN_CTAS) k_fwd_dd(DdFwdArgs
       yv = a.y + ((size_t)__ldg(a.yview + slot) * a.U + u) * a.ystride;
     }
 #pragma unroll
-    for (int s = 0; s < 4; ++s) {
-      const int z = zb * 4 + s;
-      if (z < a.zlo || z >= a.zhi) continue;
-      float val = acc[j][s] * cv;
-      if (yv) {
-        // (y - A x) / rowSum where rowSum != 0, else A x (AAPM_script/OSSART_AAPM.m:88)
-        val = rs != 0.f ? __fdiv_rn(__fsub_rn(__ldg(yv + z), val), rs) : val;
-        val *= wt;
+    for (int z = 0; z < NZ; ++z) {
+      if (!zok[z]) continue;
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        const int zs = zbk[z] * 4 + s;
+        if (zs < a.zlo || zs >= a.zhi) continue;
+        float val = acc[j][z][s] * cv;
+        if (yv) {
+          // (y - A x) / rowSum where rowSum != 0, else A x (AAPM_script/OSSART_AAPM.m:88)
+          val = rs != 0.f ? __fdiv_rn(__fsub_rn(__ldg(yv + zs), val), rs) : val;
+          val *= wt;
+        }
+        o[zs] = val;
       }
-      o[z] = val;
     }
   }
 }
@@ -208,7 +297,24 @@ struct DdAdjArgs {
   int PN, U, Z, XN, YN;
   double ocx, ocy, dx;
   BackEpi epi;
-  int zt0;
+  int zt0, nzt;
+};
+
+// pixels per thread of the direct exact adjoint
+#ifndef DDFAN_DD_BACK_VG
+#define DDFAN_DD_BACK_VG 2
+#endif
+
+// Voxel tile of the direct exact adjoint: NG = 256/ZL groups as LT lines x
+// SPL segments of VG consecutive voxels along the line.
+template <int ZL>
+struct DdBackTile {
+  static constexpr int NT = 256;
+  static constexpr int NG = NT / ZL;
+  static constexpr int VG = DDFAN_DD_BACK_VG;
+  static constexpr int SPL = 8;
+  static constexpr int KT = SPL * VG;
+  static constexpr int LT = NG / SPL;
 };
 
 // Transpose of k_fwd_dd, on the geometry of k_back_adj: pixel k of line ii
@@ -216,58 +322,76 @@ struct DdAdjArgs {
 // - Q(beta(k)), Q the channel prefix sum of w, beta the fractional boundary
 // index of a pixel edge (bracket from the fan-tangent table, fraction from the
 // FP64 boundary lines).  Here the difference is walked over w itself; a
-// thread owns VG consecutive pixels of a line, whose walks chain (the end of
-// one is the start of the next).
-template <int ZL, bool XM>
+// thread owns VG consecutive pixels of a line in NZ z-tiles, whose walks
+// chain (the end of one is the start of the next).  Every warp brackets the
+// edges of its own groups, ZL views at a time, and synchronises with itself
+// only.
+template <int ZL, bool XM, int NZ>
 __global__ void __launch_bounds__(256, DDFAN_DD_BACK_MIN_CTAS) k_back_dd(DdAdjArgs a) {
-  using T = BackTile<ZL>;
-  constexpr int NT = T::NT, VG = T::VG, SPL = T::SPL, KT = T::KT, LT = T::LT, NE = T::NE;
-  constexpr int LS = T::LS, NES = T::NES;
-  constexpr int VC = (1024 / NE) < 1 ? 1 : ((1024 / NE) > 4 ? 4 : 1024 / NE);
+  using T = DdBackTile<ZL>;
+  constexpr int NT = T::NT, VG = T::VG, SPL = T::SPL, KT = T::KT, LT = T::LT;
+  constexpr int NW = NT / 32, GW = 32 / ZL;  // warps, voxel groups per warp
+  constexpr int VCW = ZL;                    // views per warp chunk (VCW * GW = 32)
+  constexpr int NEG = VG + 1;                // edges per group
   constexpr int TBMAX = 1024, LUTMAX = 4096;
-  __shared__ int2 s_geo[VC][NES];  // edge k of line l at l * LS + k + k / VG
-  __shared__ int s_p[VC];
-  __shared__ float s_sgn[VC];
+  __shared__ int2 s_geo[NW][VCW][GW][NEG];
+  __shared__ int s_p[NW][VCW];
+  __shared__ float s_sgn[NW][VCW];
   __shared__ float s_tb[TBMAX];
   __shared__ uint16_t s_lut[LUTMAX];
-  const int tid = threadIdx.x;
-  const int zl = tid % ZL, g = tid / ZL;
-  const int zt = blockIdx.z + a.zt0;
-  const int zb = zt * ZL + zl;
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  const int zl = lane % ZL, gw = lane / ZL;
+  const int zt_first = a.zt0 + (int)blockIdx.z * NZ;
+  int zbk[NZ], zoff[NZ];
+  bool zok[NZ];
+#pragma unroll
+  for (int z = 0; z < NZ; ++z) {
+    zbk[z] = (zt_first + z) * ZL + zl;
+    zok[z] = (int)blockIdx.z * NZ + z < a.nzt && zbk[z] < a.P4;
+    zoff[z] = zok[z] ? z * ZL : 0;  // a tile past the image reads the first one again (dropped)
+  }
   const int nl = XM ? a.XN : a.YN, N = XM ? a.YN : a.XN;
   const int ntk = (N + KT - 1) / KT;
   const int tl = blockIdx.x / ntk, tk = blockIdx.x - tl * ntk;
   const int l0 = tl * LT, k0 = tk * KT;
+  const int g = w * GW + gw;  // the thread's voxel group in the tile
   const int l = g / SPL, sg = g - l * SPL;
   const int ii = l0 + l, ks = k0 + sg * VG;
-  const bool active = zb < a.P4 && ii < nl && ks < N;
+  const bool active = zok[0] && ii < nl && ks < N;
   for (int i = tid; i <= a.U; i += NT) s_tb[i] = a.tb[i];
   for (int i = tid; i < a.M; i += NT) s_lut[i] = a.lut[i];
   const int nx = a.counts[0];
   const int vbeg = XM ? 0 : nx, vend = XM ? nx : a.PN;
-  float acc[VG][4];
+  float acc[VG][NZ][4];
+  float4 vm[NZ];  // first interior values (kept between walks; see walk_nz)
 #pragma unroll
-  for (int v = 0; v < VG; ++v) acc[v][0] = acc[v][1] = acc[v][2] = acc[v][3] = 0.f;
+  for (int z = 0; z < NZ; ++z) vm[z] = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+  for (int v = 0; v < VG; ++v)
+#pragma unroll
+    for (int z = 0; z < NZ; ++z) acc[v][z][0] = acc[v][z][1] = acc[v][z][2] = acc[v][z][3] = 0.f;
   const size_t P4 = (size_t)a.P4;
   const size_t vstride = (size_t)(a.U + 1) * P4;
   const double ocl = XM ? a.ocx : a.ocy, ock = XM ? a.ocy : a.ocx;
-  __syncthreads();
+  __syncthreads();  // the bracket tables; the rest of the kernel synchronises per warp
   const float tfirst = s_tb[0], tlast = s_tb[a.U];
-  for (int v0 = vbeg; v0 < vend; v0 += VC) {
-    const int nvc = min(VC, vend - v0);
-    if (tid < VC && tid < nvc) {
-      const int p = a.order[v0 + tid];
-      s_p[tid] = p;
-      s_sgn[tid] = a.vg[p].sgn;
+  for (int v0 = vbeg; v0 < vend; v0 += VCW) {
+    const int nvc = min(VCW, vend - v0);
+    if (lane < nvc) {
+      const int p = a.order[v0 + lane];
+      s_p[w][lane] = p;
+      s_sgn[w][lane] = a.vg[p].sgn;
     }
-    for (int e = tid; e < VC * NE; e += NT) {
-      const int vv = e / NE, r = e - vv * NE;
-      const int le = r / (KT + 1), ke = r - le * (KT + 1);
-      const int li = l0 + le, ck = k0 + ke;
+    __syncwarp();
+    for (int e = lane; e < VCW * GW * NEG; e += 32) {
+      const int vv = e / (GW * NEG), r = e - vv * (GW * NEG);
+      const int gl = r / NEG, ke = r - gl * NEG;
+      const int gg = w * GW + gl;
+      const int li = l0 + gg / SPL, ck = k0 + (gg % SPL) * VG + ke;
       int b = 0;
       float frac = 0.f;
       if (vv < nvc && li < nl && ck <= N) {
-        const int p = a.order[v0 + vv];
+        const int p = s_p[w][vv];
         const ViewGeom& G = a.vg[p];
         const double lineX = (li - ocl) * a.dx, along = ((double)ck - 0.5 - ock) * a.dx;
         const float vx = (float)((XM ? lineX : along) - G.sx);
@@ -292,45 +416,45 @@ __global__ void __launch_bounds__(256, DDFAN_DD_BACK_MIN_CTAS) k_back_dd(DdAdjAr
           frac = fminf(fmaxf(frac, 0.f), 1.f);
         }
       }
-      s_geo[vv][le * LS + ke + ke / VG] = make_int2(b, __float_as_int(frac));
+      s_geo[w][vv][gl][ke] = make_int2(b, __float_as_int(frac));
     }
-    __syncthreads();
+    __syncwarp();
     if (active) {
       for (int vv = 0; vv < nvc; ++vv) {
-        const float4* base = a.w + (size_t)s_p[vv] * vstride + zb;
-        const float sgn = s_sgn[vv];
-        const int2* geo = &s_geo[vv][l * LS + sg * (VG + 1)];
+        const float4* base = a.w + (size_t)s_p[w][vv] * vstride + zbk[0];
+        const float sgn = s_sgn[w][vv];
+        const int2* geo = &s_geo[w][vv][gw][0];
         int2 gi = geo[0];
         int k = gi.x;
         float f = __int_as_float(gi.y);
-        float4 cur = __ldg(base + (size_t)k * P4);
+        float4 cur[NZ];
+        {
+          const float4* p0 = base + (size_t)k * P4;
+#pragma unroll
+          for (int z = 0; z < NZ; ++z) cur[z] = __ldg(p0 + zoff[z]);
+        }
 #pragma unroll
         for (int v = 0; v < VG; ++v) {
-          gi = geo[v + 1 == VG ? VG + 1 : v + 1];
+          gi = geo[v + 1];
           const int k1 = gi.x;
           const float f1 = __int_as_float(gi.y);
-          const float3 w = walk_weights(k, f, k1, f1, sgn);
-          fma4(acc[v], w.x, cur);
-          const int dn = k1 - k;
-          if (dn != 0) {
-            const int st = dn > 0 ? 1 : -1, n = dn > 0 ? dn : -dn;
-            for (int i = 1; i < n; ++i) fma4(acc[v], w.y, __ldg(base + (size_t)(k + i * st) * P4));
-            k = k1;
-            cur = __ldg(base + (size_t)k * P4);
-            fma4(acc[v], w.z, cur);
-          }
+          const float3 wt = walk3(k, f, k1, f1, sgn);
+          walk_nz<NZ>(acc[v], cur, vm, base, P4, zoff, k, k1, a.U, make_float4(wt.x, wt.y, wt.z, 0.f));
+          k = k1;
           f = f1;
         }
       }
     }
-    __syncthreads();
+    __syncwarp();
   }
   if (!active) return;
 #pragma unroll
   for (int v = 0; v < VG; ++v) {
     const int kk = ks + v;
     if (kk >= N) break;
-    back_store(a.epi, XM ? ii : kk, XM ? kk : ii, zb, a.XN, a.Z, true, acc[v]);
+#pragma unroll
+    for (int z = 0; z < NZ; ++z)
+      if (zok[z]) back_store(a.epi, XM ? ii : kk, XM ? kk : ii, zbk[z], a.XN, a.Z, true, acc[v][z]);
   }
 }
 
@@ -370,6 +494,7 @@ __global__ void __launch_bounds__(256, DDFAN_REF_MIN_CTAS) k_back_ref_dd(DdRefAr
   const int iy = y0 + l, ixs = x0 + sg * VG;
   const bool active = zb < a.P4 && iy < a.YN && ixs < a.XN;
   float acc[VG][4];
+  float4 vm[1] = {make_float4(0.f, 0.f, 0.f, 0.f)};  // first interior value (see walk_nz)
 #pragma unroll
   for (int v = 0; v < VG; ++v) acc[v][0] = acc[v][1] = acc[v][2] = acc[v][3] = 0.f;
   const double Ud = (double)a.U;
@@ -414,14 +539,11 @@ __global__ void __launch_bounds__(256, DDFAN_REF_MIN_CTAS) k_back_ref_dd(DdRefAr
           const int r = l * KT + sg * VG + v;
           const int2 ii = s_i[vv][r];
           const float2 ff = s_f[vv][r];
-          const float3 w = walk_weights(ii.x, ff.x, ii.y, ff.y, s_w[vv][r]);
-          fma4(acc[v], w.x, __ldg(base + (size_t)ii.x * P4));
-          const int dn = ii.y - ii.x;
-          if (dn != 0) {
-            const int st = dn > 0 ? 1 : -1, n = dn > 0 ? dn : -dn;
-            for (int i = 1; i < n; ++i) fma4(acc[v], w.y, __ldg(base + (size_t)(ii.x + i * st) * P4));
-            fma4(acc[v], w.z, __ldg(base + (size_t)ii.y * P4));
-          }
+          const float3 wt = walk3(ii.x, ff.x, ii.y, ff.y, s_w[vv][r]);
+          float4 cur[1] = {__ldg(base + (size_t)ii.x * P4)};
+          const int zo[1] = {0};
+          walk_nz<1>(reinterpret_cast<float(&)[1][4]>(acc[v]), cur, vm, base, P4, zo, ii.x, ii.y, a.U,
+                     make_float4(wt.x, wt.y, wt.z, 0.f));
         }
       }
     }
