@@ -53,6 +53,10 @@ SIGNATURES = {
     "ddfan_ossart_image_ptr": (_p, [_p]),
     "ddfan_ossart_launches_per_iter": (_i, [_p]),
     "ddfan_ossart_profile": (_i, [_p, _i, _p, _p, _p]),
+    "ddfan_batch_create": (_i, [_p, _p, _i]),
+    "ddfan_batch_destroy": (None, [_p]),
+    "ddfan_batch_iterate": (_i, [_p, _i, _i, _p]),
+    "ddfan_batch_launches_per_iter": (_i, [_p]),
     "ddfan_OSSART_AAPM": (_i, [_f, _f, _i, _p, _p, _f, _f, _f, _p, _p, _i, _i, _i, _i, _f, _p, _p, _i,
                                _i, _i, _i, _i, _i, _p]),
     "ddfan_HelicalToFan": (_i, [_p, _p, _p, _ll, _p, _i, _f, _f, _f, _i, _i, _f, _f, _i, _f, _f]),

@@ -10,9 +10,9 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libddfan.so")
-SOURCES = ["ddfan.cu", "ddfan_solver.cu", "ddfan_ps.cu", "ddfan_noalloc.cu", "ddfan_rebin.cu"]
+SOURCES = ["ddfan.cu", "ddfan_solver.cu", "ddfan_ps.cu", "ddfan_noalloc.cu", "ddfan_rebin.cu", "ddfan_batch.cu"]
 HEADERS = ["ddfan_device.cuh", "ddfan_kernels.cuh", "ddfan_proj_kernels.cuh", "ddfan_plan.h", "ddfan_ps.h",
-           "ddfan_ps_kernels.cuh", "ddfan_dd_kernels.cuh"]
+           "ddfan_ps_kernels.cuh", "ddfan_dd_kernels.cuh", "ddfan_solver.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

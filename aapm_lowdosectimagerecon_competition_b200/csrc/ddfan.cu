@@ -621,18 +621,6 @@ int launch_publish_masked(const float* x, int Zi, const float* x0, int Z, const 
   return check_launch("k_publish_masked");
 }
 
-// channels per thread of the direct forward projector for a z-lane count
-#ifndef DDFAN_DD_FWD_CG
-#define DDFAN_DD_FWD_CG 1
-#endif
-template <int ZL> struct DdFwdCG { static constexpr int v = ZL >= 4 ? DDFAN_DD_FWD_CG : (ZL == 2 ? 2 : 1); };
-
-// z-tiles per thread of the direct kernels: each decoded footprint serves
-// 4 slices per z-tile, so more z-tiles per thread means fewer instructions
-// per slice (the measured lever: 1 -> 4 took a 96-view c3 subset's forward
-// from 3.5 to 2.6 ms); at most the call's z-tiles
-static int dd_nz(int nzt) { return nzt >= 4 && DDFAN_DD_NZ >= 4 ? 4 : (nzt >= 2 && DDFAN_DD_NZ >= 2 ? 2 : 1); }
-
 template <int ZL>
 static void fwd_dd_go(const DdFwdArgs& a, int nzt, cudaStream_t st) {
   constexpr int CG = DdFwdCG<ZL>::v;
@@ -654,9 +642,9 @@ static void fwd_dd_go(const DdFwdArgs& a, int nzt, cudaStream_t st) {
   }
 }
 
-int launch_fwd_dd(const Plan& p, const float* img, const ViewGeom* vg, const double2* fc, const float* cvd,
-                  const int* order, int PN, float* out, int orow, int ostride, int zlo, int zhi,
-                  const DdResidual* res, cudaStream_t st) {
+DdFwdArgs make_fwd_dd_args(const Plan& p, const float* img, const ViewGeom* vg, const double2* fc,
+                           const float* cvd, const int* order, int PN, float* out, int orow, int ostride, int zlo,
+                           int zhi, const DdResidual* res) {
   DdFwdArgs a{};
   a.img = reinterpret_cast<const float4*>(img); a.P4 = p.P4;
   a.vg = vg; a.fc = fc; a.cvd = cvd; a.order = order;
@@ -666,9 +654,15 @@ int launch_fwd_dd(const Plan& p, const float* img, const ViewGeom* vg, const dou
   if (res) {
     a.y = res->y; a.yview = res->yview; a.rowsum = res->rowsum; a.wgt = res->wgt; a.ystride = res->ystride;
   }
-  int nzt = 0;
-  ztile_range(p, zlo, zhi, &a.zt0, &nzt);
-  a.nzt = nzt;
+  ztile_range(p, zlo, zhi, &a.zt0, &a.nzt);
+  return a;
+}
+
+int launch_fwd_dd(const Plan& p, const float* img, const ViewGeom* vg, const double2* fc, const float* cvd,
+                  const int* order, int PN, float* out, int orow, int ostride, int zlo, int zhi,
+                  const DdResidual* res, cudaStream_t st) {
+  const DdFwdArgs a = make_fwd_dd_args(p, img, vg, fc, cvd, order, PN, out, orow, ostride, zlo, zhi, res);
+  const int nzt = a.nzt;
   if (nzt == 0 || PN < 1) return DDFAN_OK;
   ProfScope ps(KIND_FWD, st);
   switch (p.ZL) {
@@ -709,11 +703,11 @@ static void ref_dd_go(const DdRefArgs& a, int nzt, cudaStream_t st) {
   k_back_ref_dd<ZL><<<dim3(tiles, 1, nzt), T::NT, 0, st>>>(a);
 }
 
-int launch_back_dd(const Plan& p, int back_mode, const float* w, const ViewGeom* vg, const double2* fc,
-                   const int* order, const int* counts, int PN, const BackEpi& epi, cudaStream_t st) {
+int make_back_dd_args(const Plan& p, int back_mode, const float* w, const ViewGeom* vg, const double2* fc,
+                      const int* order, const int* counts, int PN, const BackEpi& epi, DdAdjArgs* pass1,
+                      DdAdjArgs* pass2, DdRefArgs* ref) {
   int zt0 = 0, nzt = 0;
   ztile_range(p, epi.zlo, epi.zhi, &zt0, &nzt);
-  if (nzt == 0 || PN < 1) return DDFAN_OK;
   if (back_mode == DDFAN_BACK_REF) {
     DdRefArgs a{};
     a.q = reinterpret_cast<const float4*>(w); a.P4 = p.P4; a.vg = vg;
@@ -722,19 +716,9 @@ int launch_back_dd(const Plan& p, int back_mode, const float* w, const ViewGeom*
     a.inv_sid = p.inv_sid; a.inv_dbeta = p.inv_dbeta; a.cnt = (double)p.detCntIdx + 0.5;
     a.epi = epi;
     a.zt0 = zt0;
-    ProfScope ps(KIND_BACK_A, st);
-    switch (p.ZL) {
-      case 8: ref_dd_go<8>(a, nzt, st); break;
-      case 4: ref_dd_go<4>(a, nzt, st); break;
-      case 2: ref_dd_go<2>(a, nzt, st); break;
-      default: ref_dd_go<1>(a, nzt, st); break;
-    }
-    return check_launch("k_back_ref_dd");
+    *ref = a;
+    return nzt;
   }
-  if (back_mode != DDFAN_BACK_ADJ) return set_err(DDFAN_ERR_ARG, "back_mode %d", back_mode);
-  if (!p.adj_ok) return set_err(DDFAN_ERR_UNSUPPORTED, "detector boundaries are not monotone as seen from the source");
-  if (!order || !counts) return set_err(DDFAN_ERR_ARG, "exact adjoint needs the view order");
-  if (p.U + 1 > 1024 || p.M > 4096) return set_err(DDFAN_ERR_UNSUPPORTED, "exact adjoint: %d channels", p.U);
   DdAdjArgs a{};
   a.w = reinterpret_cast<const float4*>(w); a.P4 = p.P4;
   a.vg = vg; a.fc = fc; a.tb = p.d_tb; a.lut = p.d_lut;
@@ -745,21 +729,53 @@ int launch_back_dd(const Plan& p, int back_mode, const float* w, const ViewGeom*
   a.zt0 = zt0;
   a.nzt = nzt;
   // pass 1: x-major views along x columns -> tmp (mask applied)
-  a.epi = epi;
-  a.epi.out = p.d_tmp; a.epi.addend = nullptr; a.epi.xin = nullptr; a.epi.colsum = nullptr;
-  a.epi.nonneg = 0;
+  *pass1 = a;
+  pass1->epi = epi;
+  pass1->epi.out = p.d_tmp; pass1->epi.addend = nullptr; pass1->epi.xin = nullptr; pass1->epi.colsum = nullptr;
+  pass1->epi.nonneg = 0;
+  // pass 2: y-major views along y rows, plus pass 1, then the final epilogue
+  *pass2 = a;
+  pass2->epi = epi;
+  pass2->epi.addend = p.d_tmp;
+  return nzt;
+}
+
+int check_back_dd(const Plan& p, int back_mode, const int* order, const int* counts) {
+  if (back_mode == DDFAN_BACK_REF) return DDFAN_OK;
+  if (back_mode != DDFAN_BACK_ADJ) return set_err(DDFAN_ERR_ARG, "back_mode %d", back_mode);
+  if (!p.adj_ok) return set_err(DDFAN_ERR_UNSUPPORTED, "detector boundaries are not monotone as seen from the source");
+  if (!order || !counts) return set_err(DDFAN_ERR_ARG, "exact adjoint needs the view order");
+  if (p.U + 1 > 1024 || p.M > 4096) return set_err(DDFAN_ERR_UNSUPPORTED, "exact adjoint: %d channels", p.U);
+  return DDFAN_OK;
+}
+
+int launch_back_dd(const Plan& p, int back_mode, const float* w, const ViewGeom* vg, const double2* fc,
+                   const int* order, const int* counts, int PN, const BackEpi& epi, cudaStream_t st) {
+  int rc = check_back_dd(p, back_mode, order, counts);
+  if (rc) return rc;
+  DdAdjArgs a1, a2;
+  DdRefArgs ar;
+  const int nzt = make_back_dd_args(p, back_mode, w, vg, fc, order, counts, PN, epi, &a1, &a2, &ar);
+  if (nzt == 0 || PN < 1) return DDFAN_OK;
+  if (back_mode == DDFAN_BACK_REF) {
+    ProfScope ps(KIND_BACK_A, st);
+    switch (p.ZL) {
+      case 8: ref_dd_go<8>(ar, nzt, st); break;
+      case 4: ref_dd_go<4>(ar, nzt, st); break;
+      case 2: ref_dd_go<2>(ar, nzt, st); break;
+      default: ref_dd_go<1>(ar, nzt, st); break;
+    }
+    return check_launch("k_back_ref_dd");
+  }
   {
     ProfScope ps(KIND_BACK_A, st);
-    back_dd_zl<true>(p.ZL, a, nzt, st);
+    back_dd_zl<true>(p.ZL, a1, nzt, st);
   }
-  int rc = check_launch("k_back_dd<x>");
+  rc = check_launch("k_back_dd<x>");
   if (rc) return rc;
-  // pass 2: y-major views along y rows, plus pass 1, then the final epilogue
-  a.epi = epi;
-  a.epi.addend = p.d_tmp;
   {
     ProfScope ps(KIND_BACK_B, st);
-    back_dd_zl<false>(p.ZL, a, nzt, st);
+    back_dd_zl<false>(p.ZL, a2, nzt, st);
   }
   return check_launch("k_back_dd<y>");
 }

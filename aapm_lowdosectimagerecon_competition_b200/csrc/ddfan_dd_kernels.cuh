@@ -140,6 +140,18 @@ struct DdFwdArgs {
 #define DDFAN_DD_NZ 4
 #endif
 
+// channels per thread of the direct forward projector for a z-lane count
+#ifndef DDFAN_DD_FWD_CG
+#define DDFAN_DD_FWD_CG 1
+#endif
+template <int ZL> struct DdFwdCG { static constexpr int v = ZL >= 4 ? DDFAN_DD_FWD_CG : (ZL == 2 ? 2 : 1); };
+
+// z-tiles per thread of the direct kernels: each decoded footprint serves
+// 4 slices per z-tile, so more z-tiles per thread means fewer instructions
+// per slice (the measured lever: 1 -> 4 took a 96-view c3 subset's forward
+// from 3.5 to 2.6 ms); at most the call's z-tiles
+inline int dd_nz(int nzt) { return nzt >= 4 && DDFAN_DD_NZ >= 4 ? 4 : (nzt >= 2 && DDFAN_DD_NZ >= 2 ? 2 : 1); }
+
 template <int ZL, int CG, int NZ>
 struct DdFwdTile {
   static constexpr int NT = 256, NW = NT / 32;
@@ -158,27 +170,26 @@ struct DdFwdTile {
 // 1 / footprint length, MultiSlicesProjGPU.cu:166-170) and synchronises with
 // itself only, so warps interleave FP64 geometry with other warps' gathers.
 template <int ZL, int CG, int NZ>
-__global__ void __launch_bounds__(256, DDFAN_DD_FWD_MIN_CTAS) k_fwd_dd(DdFwdArgs a) {
+__device__ __forceinline__ void fwd_dd_body(const DdFwdArgs& a, int row, int cblk, int zgrp) {
   using T = DdFwdTile<ZL, CG, NZ>;
   constexpr int NW = T::NW, CWW = T::CWW, CW = T::CW, CC = T::CC;
   __shared__ double2 s_fc[NW][CWW + 1];
   __shared__ float4 s_w[NW][CC][CWW];  // (w0, wm, we) / length; k0 | k1 << 16 as int bits
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
   const int zl = lane % ZL, gw = lane / ZL;
-  const int row = a.row0 + (int)blockIdx.y;
   if (row >= a.PN) return;  // uniform per CTA
   const int slot = a.order ? a.order[row] : row;
   const int p = slot;
-  const int wc0 = blockIdx.x * CW + w * CWW;  // the warp's first channel
+  const int wc0 = cblk * CW + w * CWW;  // the warp's first channel
   if (wc0 >= a.U) return;  // uniform per warp; no CTA-wide barrier follows
-  // z-tiles zt0 + blockIdx.z * NZ + z of the call's nzt; block zb = zt * ZL + zl
-  const int zt_first = a.zt0 + (int)blockIdx.z * NZ;
+  // z-tiles zt0 + zgrp * NZ + z of the call's nzt; block zb = zt * ZL + zl
+  const int zt_first = a.zt0 + zgrp * NZ;
   int zbk[NZ], zoff[NZ];
   bool zok[NZ];
 #pragma unroll
   for (int z = 0; z < NZ; ++z) {
     zbk[z] = (zt_first + z) * ZL + zl;
-    zok[z] = (int)blockIdx.z * NZ + z < a.nzt && zbk[z] < a.P4;
+    zok[z] = zgrp * NZ + z < a.nzt && zbk[z] < a.P4;
     zoff[z] = zok[z] ? z * ZL : 0;  // a tile past the image reads the first one again (dropped)
   }
   const bool xm = a.vg[p].xmajor != 0;
@@ -281,6 +292,21 @@ __global__ void __launch_bounds__(256, DDFAN_DD_FWD_MIN_CTAS) k_fwd_dd(DdFwdArgs
   }
 }
 
+// One CTA per (view row, channel block, z-tile group) of one call.
+template <int ZL, int CG, int NZ>
+__global__ void __launch_bounds__(256, DDFAN_DD_FWD_MIN_CTAS) k_fwd_dd(const __grid_constant__ DdFwdArgs a) {
+  fwd_dd_body<ZL, CG, NZ>(a, a.row0 + (int)blockIdx.y, (int)blockIdx.x, (int)blockIdx.z);
+}
+
+// One launch over a work list of many calls (batched reconstructions): CTA
+// b takes item {call, view row, channel block, z-tile group} = items[b].
+template <int ZL, int CG, int NZ>
+__global__ void __launch_bounds__(256, DDFAN_DD_FWD_MIN_CTAS) k_fwd_dd_batch(const DdFwdArgs* __restrict__ args,
+                                                                              const int4* __restrict__ items) {
+  const int4 it = items[blockIdx.x];
+  fwd_dd_body<ZL, CG, NZ>(args[it.x], it.y, it.z, it.w);
+}
+
 // ============================================================ exact adjoint
 
 struct DdAdjArgs {
@@ -327,7 +353,7 @@ struct DdBackTile {
 // edges of its own groups, ZL views at a time, and synchronises with itself
 // only.
 template <int ZL, bool XM, int NZ>
-__global__ void __launch_bounds__(256, DDFAN_DD_BACK_MIN_CTAS) k_back_dd(DdAdjArgs a) {
+__device__ __forceinline__ void back_dd_body(const DdAdjArgs& a, int tile, int zgrp) {
   using T = DdBackTile<ZL>;
   constexpr int NT = T::NT, VG = T::VG, SPL = T::SPL, KT = T::KT, LT = T::LT;
   constexpr int NW = NT / 32, GW = 32 / ZL;  // warps, voxel groups per warp
@@ -341,18 +367,18 @@ __global__ void __launch_bounds__(256, DDFAN_DD_BACK_MIN_CTAS) k_back_dd(DdAdjAr
   __shared__ uint16_t s_lut[LUTMAX];
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
   const int zl = lane % ZL, gw = lane / ZL;
-  const int zt_first = a.zt0 + (int)blockIdx.z * NZ;
+  const int zt_first = a.zt0 + zgrp * NZ;
   int zbk[NZ], zoff[NZ];
   bool zok[NZ];
 #pragma unroll
   for (int z = 0; z < NZ; ++z) {
     zbk[z] = (zt_first + z) * ZL + zl;
-    zok[z] = (int)blockIdx.z * NZ + z < a.nzt && zbk[z] < a.P4;
+    zok[z] = zgrp * NZ + z < a.nzt && zbk[z] < a.P4;
     zoff[z] = zok[z] ? z * ZL : 0;  // a tile past the image reads the first one again (dropped)
   }
   const int nl = XM ? a.XN : a.YN, N = XM ? a.YN : a.XN;
   const int ntk = (N + KT - 1) / KT;
-  const int tl = blockIdx.x / ntk, tk = blockIdx.x - tl * ntk;
+  const int tl = tile / ntk, tk = tile - tl * ntk;
   const int l0 = tl * LT, k0 = tk * KT;
   const int g = w * GW + gw;  // the thread's voxel group in the tile
   const int l = g / SPL, sg = g - l * SPL;
@@ -458,6 +484,20 @@ __global__ void __launch_bounds__(256, DDFAN_DD_BACK_MIN_CTAS) k_back_dd(DdAdjAr
   }
 }
 
+// One CTA per (voxel tile, z-tile group) of one call.
+template <int ZL, bool XM, int NZ>
+__global__ void __launch_bounds__(256, DDFAN_DD_BACK_MIN_CTAS) k_back_dd(const __grid_constant__ DdAdjArgs a) {
+  back_dd_body<ZL, XM, NZ>(a, (int)blockIdx.x, (int)blockIdx.z);
+}
+
+// The work-list launch: CTA b takes item {call, voxel tile, z-tile group} = items[b].
+template <int ZL, bool XM, int NZ>
+__global__ void __launch_bounds__(256, DDFAN_DD_BACK_MIN_CTAS) k_back_dd_batch(const DdAdjArgs* __restrict__ args,
+                                                                                const int4* __restrict__ items) {
+  const int4 it = items[blockIdx.x];
+  back_dd_body<ZL, XM, NZ>(args[it.x], it.y, it.z);
+}
+
 // ============================================================ reference backprojector
 
 struct DdRefArgs {
@@ -475,7 +515,7 @@ struct DdRefArgs {
 // tile); the difference of the two channel prefix-sum samples is walked over
 // the residual itself.
 template <int ZL>
-__global__ void __launch_bounds__(256, DDFAN_REF_MIN_CTAS) k_back_ref_dd(DdRefArgs a) {
+__device__ __forceinline__ void ref_dd_body(const DdRefArgs& a, int tile, int ztg) {
   using T = BackTile<ZL>;
   constexpr int NT = T::NT, VG = T::VG, SPL = T::SPL, KT = T::KT, LT = T::LT, NV = T::NV;
   constexpr int VC = (2048 / NV) < 1 ? 1 : ((2048 / NV) > 4 ? 4 : 2048 / NV);
@@ -485,10 +525,10 @@ __global__ void __launch_bounds__(256, DDFAN_REF_MIN_CTAS) k_back_ref_dd(DdRefAr
   __shared__ int s_p[VC];
   const int tid = threadIdx.x;
   const int zl = tid % ZL, g = tid / ZL;
-  const int zt = blockIdx.z + a.zt0;
+  const int zt = ztg + a.zt0;
   const int zb = zt * ZL + zl;
   const int ntx = (a.XN + KT - 1) / KT;
-  const int ty = blockIdx.x / ntx, tx = blockIdx.x - ty * ntx;
+  const int ty = tile / ntx, tx = tile - ty * ntx;
   const int y0 = ty * LT, x0 = tx * KT;
   const int l = g / SPL, sg = g - l * SPL;
   const int iy = y0 + l, ixs = x0 + sg * VG;
@@ -553,6 +593,20 @@ __global__ void __launch_bounds__(256, DDFAN_REF_MIN_CTAS) k_back_ref_dd(DdRefAr
 #pragma unroll
   for (int v = 0; v < VG; ++v)
     if (ixs + v < a.XN) back_store(a.epi, ixs + v, iy, zb, a.XN, a.Z, false, acc[v]);
+}
+
+// One CTA per (voxel tile, z-tile) of one call.
+template <int ZL>
+__global__ void __launch_bounds__(256, DDFAN_REF_MIN_CTAS) k_back_ref_dd(const __grid_constant__ DdRefArgs a) {
+  ref_dd_body<ZL>(a, (int)blockIdx.x, (int)blockIdx.z);
+}
+
+// The work-list launch: CTA b takes item {call, voxel tile, z-tile} = items[b].
+template <int ZL>
+__global__ void __launch_bounds__(256, DDFAN_REF_MIN_CTAS) k_back_ref_dd_batch(const DdRefArgs* __restrict__ args,
+                                                                                const int4* __restrict__ items) {
+  const int4 it = items[blockIdx.x];
+  ref_dd_body<ZL>(args[it.x], it.y, it.z);
 }
 
 // ============================================================ staging

@@ -275,4 +275,34 @@ static __global__ void k_fista_t(double* t0p) {
   *t0p = (1.0 + sqrt(1.0 + 4.0 * t0 * t0)) / 2.0;
 }
 
+// The same for many solves in one launch pair: blockIdx.y is the solve.
+struct FistaDesc {
+  float* x;
+  float* xprev;
+  size_t n;
+  double* t;
+};
+
+static __global__ void k_fista_batch(const FistaDesc* __restrict__ d) {
+  const FistaDesc f = d[blockIdx.y];
+  const double t0 = *f.t;
+  const double t1 = (1.0 + sqrt(1.0 + 4.0 * t0 * t0)) / 2.0;
+  const float mom = (float)((t0 - 1.0) / t1);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < f.n; i += (size_t)gridDim.x * blockDim.x) {
+    const float xv = f.x[i];
+    const float v = xv + mom * (xv - f.xprev[i]);
+    f.x[i] = v;
+    f.xprev[i] = v;
+  }
+}
+
+static __global__ void k_fista_t_batch(const FistaDesc* __restrict__ d, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    double* tp = d[i].t;
+    const double t0 = *tp;
+    *tp = (1.0 + sqrt(1.0 + 4.0 * t0 * t0)) / 2.0;
+  }
+}
+
 }  // namespace ddfan

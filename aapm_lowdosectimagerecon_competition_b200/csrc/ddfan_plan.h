@@ -11,6 +11,9 @@
 namespace ddfan {
 
 struct BackEpi;
+struct DdFwdArgs;
+struct DdAdjArgs;
+struct DdRefArgs;
 
 int set_err(int code, const char* fmt, ...);
 const char* last_error();
@@ -136,6 +139,17 @@ struct DdResidual {
 int launch_fwd_dd(const Plan& p, const float* img, const ViewGeom* vg, const double2* fc, const float* cvd,
                   const int* order, int PN, float* out, int orow, int ostride, int zlo, int zhi,
                   const DdResidual* res, cudaStream_t st);
+// The arguments launch_fwd_dd would launch with (nzt: z-tiles of [zlo, zhi)).
+DdFwdArgs make_fwd_dd_args(const Plan& p, const float* img, const ViewGeom* vg, const double2* fc,
+                           const float* cvd, const int* order, int PN, float* out, int orow, int ostride, int zlo,
+                           int zhi, const DdResidual* res);
+// The arguments launch_back_dd would launch with: the exact adjoint's two
+// passes, or the REF backprojector's one; returns the z-tile count.
+int make_back_dd_args(const Plan& p, int back_mode, const float* w, const ViewGeom* vg, const double2* fc,
+                      const int* order, const int* counts, int PN, const BackEpi& epi, DdAdjArgs* pass1,
+                      DdAdjArgs* pass2, DdRefArgs* ref);
+// what launch_back_dd checks before launching (status code)
+int check_back_dd(const Plan& p, int back_mode, const int* order, const int* counts);
 // Backprojection of w [slot][U+1][4 P4] (guard channel U = 0; weighted by
 // 1/|dir.axis| for the exact adjoint) with the epilogue `epi`.
 int launch_back_dd(const Plan& p, int back_mode, const float* w, const ViewGeom* vg, const double2* fc,

@@ -179,11 +179,10 @@ template <> struct AccS<SAT_FP64> {
 // 32-bit words of a cell's prefix sum
 template <int M> struct PsInfo { static constexpr int SW = M == SAT_FP32 ? 1 : 2; };
 
-__device__ __forceinline__ float rcp_approx(float x) {
-  float r;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-  return r;
-}
+// Correctly rounded reciprocal (IEEE round-to-nearest) of the footprint
+// length and of the bracket width: an approximate one moved row sums by ~1e-7
+// between kernels, which an OS-SART solve amplifies.
+__device__ __forceinline__ float rcp_exact(float x) { return __frcp_rn(x); }
 
 // ---------------------------------------------------------------- transposes
 
@@ -349,7 +348,7 @@ __global__ void __launch_bounds__(256) k_ps_fwd(PsFwdArgs a) {
       PhiS<M> cur;
       cur.load(line + i0, f);
       const PhiS<M> nxt = cur.down();
-      part = fmaf(nxt.diff(cur), rcp_approx(fmaf(fi, lF, lC)), part);
+      part = fmaf(nxt.diff(cur), rcp_exact(fmaf(fi, lF, lC)), part);
       cf += dcf;
       fi += 1.f;
       line += Nw;
@@ -446,7 +445,7 @@ __global__ void __launch_bounds__(256) k_ps_back_adj(PsBackArgs a) {
         f0 = line_at(b);
         c0 = fma(di, f0.x, f0.y);
       }
-      const float frac = fminf(fmaxf((float)(dk - c0) * rcp_approx((float)(c1 - c0)), 0.f), 1.f);
+      const float frac = fminf(fmaxf((float)(dk - c0) * rcp_exact((float)(c1 - c0)), 0.f), 1.f);
       PhiS<M> q;
       q.load(qrow + b, frac);
       return q;

@@ -6,6 +6,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -15,6 +17,7 @@
 #include "ddfan_kernels.cuh"
 #include "ddfan_plan.h"
 #include "ddfan_ps.h"
+#include "ddfan_solver.h"
 
 namespace ddfan {
 
@@ -108,6 +111,12 @@ static int mex_slab(bool forward, const PlanDesc& d, const float* angs, int PN, 
   return DDFAN_OK;
 }
 
+// Slabs [startIdx[k], startIdx[k+1]) go to device k mod (device count); as
+// the reference does (one std::thread per GPU, AAPM_script/
+// MultiSlicesProjGPU.cu:474-484, MultiSlicesBackGPU.cu:335-347) each device's
+// slabs run on a host thread of their own, so devices work at the same time.
+// DDFAN_SLAB_THREADS=slab gives every slab its own thread (several on one
+// device: the library is thread-safe per plan and stream).
 static int mex_call(bool forward, float x0, float y0, int DNU, const float* xds, const float* yds,
                     float detCntIdx, float imgXCenter, float imgYCenter, const float* hangs, int PN,
                     int XN, int YN, int SLN, const float* in, float dx, const uint8_t* mask,
@@ -120,92 +129,56 @@ static int mex_call(bool forward, float x0, float y0, int DNU, const float* xds,
   const int ndev = device_count();
   if (ndev < 1) return set_err(DDFAN_ERR_CUDA, "no CUDA device");
   const size_t npix = (size_t)XN * YN, nray = (size_t)PN * DNU;
-  for (size_t k = 0; k < slabs.size(); ++k) {
+  auto run_slab = [&](size_t k) -> int {
     const int a = slabs[k].first, b = slabs[k].second, n = b - a;
     PlanDesc d{x0, y0, DNU, xds, yds, detCntIdx, imgXCenter, imgYCenter, XN, YN, dx, mask, n, PN,
                sat_mode, (int)(k % ndev)};
-    if (n == SLN) {
-      rc = mex_slab(forward, d, hangs, PN, in, out, back_mode);
-    } else {
-      std::vector<float> sin, sang, sout(forward ? nray * n : npix * n);
-      gather_slab(in, forward ? npix : nray, SLN, a, b, sin);
-      gather_slab(hangs, PN, SLN, a, b, sang);
-      rc = mex_slab(forward, d, sang.data(), PN, sin.data(), sout.data(), back_mode);
-      if (!rc) scatter_slab(sout, forward ? nray : npix, SLN, a, b, out);
-    }
-    if (rc) return rc;
+    if (n == SLN) return mex_slab(forward, d, hangs, PN, in, out, back_mode);
+    std::vector<float> sin, sang, sout(forward ? nray * n : npix * n);
+    gather_slab(in, forward ? npix : nray, SLN, a, b, sin);
+    gather_slab(hangs, PN, SLN, a, b, sang);
+    const int r = mex_slab(forward, d, sang.data(), PN, sin.data(), sout.data(), back_mode);
+    if (!r) scatter_slab(sout, forward ? nray : npix, SLN, a, b, out);  // disjoint slices of out
+    return r;
+  };
+  // slab groups: per device, or per slab
+  const char* ev = getenv("DDFAN_SLAB_THREADS");
+  const bool per_slab = ev && !std::strcmp(ev, "slab");
+  std::vector<std::vector<size_t>> groups;
+  if (per_slab) {
+    for (size_t k = 0; k < slabs.size(); ++k) groups.push_back({k});
+  } else {
+    groups.resize(std::min<size_t>(slabs.size(), (size_t)ndev));
+    for (size_t k = 0; k < slabs.size(); ++k) groups[k % ndev].push_back(k);
   }
+  if (groups.size() == 1) {
+    for (size_t k : groups[0])
+      if ((rc = run_slab(k))) return rc;
+    return DDFAN_OK;
+  }
+  // errors are per thread (ddfan_last_error is thread-local): carry them back
+  std::vector<int> rcs(groups.size(), DDFAN_OK);
+  std::vector<std::string> msgs(groups.size());
+  std::vector<std::thread> threads;
+  for (size_t g = 0; g < groups.size(); ++g)
+    threads.emplace_back([&, g] {
+      for (size_t k : groups[g]) {
+        const int r = run_slab(k);
+        if (r) {
+          rcs[g] = r;
+          msgs[g] = last_error();
+          return;
+        }
+      }
+    });
+  for (std::thread& t : threads) t.join();
+  for (size_t g = 0; g < groups.size(); ++g)
+    if (rcs[g]) return set_err(rcs[g], "%s", msgs[g].c_str());
   return DDFAN_OK;
 }
 
 // ====================================================================== solver
 
-struct Solver {
-  Plan* P = nullptr;  // Zi slices, PNmax = largest subset (or largest tile view range)
-  int device = 0;
-  int PNall = 0, nsub = 1, useFISTA = 1, nonneg = 0, back_mode = DDFAN_BACK_REF;
-  int XN = 0, YN = 0, U = 0, Z = 0;
-  std::vector<int> off, cnt;  // subset k: rows [off[k], off[k] + cnt[k]) of the subset-ordered tables
-  ViewGeom* d_vg = nullptr;
-  double2* d_fc = nullptr;
-  float* d_cvd = nullptr;
-  int* d_yview = nullptr;  // subset-ordered row -> original view index
-  int* d_order = nullptr;  // per subset (or per subset and z-tile): views in dispatch order (x-major first)
-  int* d_counts = nullptr; // per subset: {x-major views, others}
-  float* d_rows = nullptr; // [PNall][U]   row sums, subset order
-  float* d_cols = nullptr; // [nsub][YN][XN] column sums
-  float* d_y = nullptr;    // [PNall][U][Zi] measured sinogram
-  float* d_x = nullptr;    // [YN][XN][Zi] image
-  float* d_xprev = nullptr;
-  float* d_ax = nullptr;   // [PNmax][U][Zi]
-  double* d_t = nullptr;
-  // Per-slice view angles ("windowed" solver).  Every slice's list is a
-  // window of one table of raw views (view ib of slice z is raw view
-  // off_z + ib): the geometry rows are raw views, grouped by raw view mod
-  // numOfOS (row = (g mod nOS) * Mc + g / nOS).  Internally slices are
-  // reordered so that a z-tile holds slices of one residue off_z mod nOS --
-  // they then need the same raw views for each subset -- and each class is
-  // padded to whole z-tiles; z-tile zt of subset k projects the raw views of
-  // its residue class that fall in its slices' windows.
-  bool win = false;
-  int Zi = 0;                // internal slices (Z when not windowed)
-  int nzt = 0, Mc = 1;
-  std::vector<int> perm;     // internal slice -> original slice, -1 for padding
-  int* d_perm = nullptr;     // the same on the device
-  int* d_inv = nullptr;      // original slice -> internal slice
-  int* d_soff = nullptr;     // internal slice -> window offset (INT_MAX for padding)
-  int4* d_ztd = nullptr;     // [nsub][nzt] view ranges
-  std::vector<int> maxcnt;   // per subset: largest range of a z-tile
-  float* d_xu = nullptr;     // [YN][XN][Z] image in the caller's layout
-  float* d_stage = nullptr;  // [PNall][U][Z] host sinogram staging (windowed, slice-major)
-  // Per-slice view angles, slice-major path: every slice keeps its own
-  // geometry (rows z * cstride + m: view k + m * numOfOS of slice z in
-  // subset k, rebuilt per subset) and the image, sinogram and prefix-sum
-  // tables are slice-major: d_x [Z][YN][XN], d_y [Z][PNall][U],
-  // d_ax [Z][cstride][U].
-  bool ps = false;
-  int cstride = 0;
-  float* d_pang = nullptr;   // [nsub][Z][cstride] angles of each slice's views per subset
-  float* d_xt = nullptr;     // [Z][XN][YN] image columns
-  float* d_tabx = nullptr;   // image rows table [Z][YN][XN] cells
-  float* d_taby = nullptr;   // image columns table [Z][XN][YN] cells
-  float* d_sq = nullptr;     // weighted residual table [Z][cstride][U+1] cells
-  // Direct mode (no prefix-sum tables; one angle list for all slices): the
-  // image d_x [YN][XN][Zi] has its slices padded to a multiple of 4 (Zi) and
-  // its masked voxels kept at 0, so the projector reads it as it is; d_ax holds
-  // the residual [PNmax][U+1][Zi] with a zero guard channel.  A masked voxel's
-  // published value is its initial one (d_x0, the caller's layout), clamped
-  // at 0 by the updates when they clamp -- what the table path computes there.
-  bool direct = false;
-  float* d_x0 = nullptr;
-  long long iters_done = 0;
-  cudaStream_t own = nullptr;
-  cudaEvent_t last_use = nullptr;  // recorded after work enqueued on a caller's stream
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t gexec = nullptr;
-  size_t bytes = 0;
-  int launches = 0;
-};
 
 static void solver_free(Solver* s) {
   if (!s) return;
@@ -415,6 +388,13 @@ static int solver_publish(Solver& s, cudaStream_t st) {
                                  s.d_xu, (size_t)s.XN * s.YN, st);
   if (!remapped(s)) return DDFAN_OK;
   return gather_slices(s.d_x, s.Zi, s.d_xu, s.Z, s.d_inv, (size_t)s.XN * s.YN, st);
+}
+
+int solver_after_iterations(Solver& s, int n, cudaStream_t st) {
+  s.iters_done += n;
+  int rc = solver_publish(s, st);
+  if (!rc) cudaEventRecord(s.last_use, st);
+  return rc;
 }
 
 // Every slice's angle list as a window of one raw-view table: view ib of

@@ -173,3 +173,37 @@ class OSSART:
             self.close()
         except Exception:
             pass
+
+
+class OSSARTBatch:
+    """Many device-resident OS-SART solves advanced together
+    (ddfan_batch_*): every iteration runs each solve's next iteration with one
+    launch per kernel kind, subset step and tile class over all of them.  The
+    solvers (OSSART objects in the direct mode, one angle list each) must
+    outlive the batch; set their sinograms and images first."""
+
+    def __init__(self, solvers):
+        load()
+        self.solvers = list(solvers)
+        arr = (ctypes.c_void_p * len(self.solvers))(*[sv._h.value for sv in self.solvers])
+        h = ctypes.c_void_p()
+        call("ddfan_batch_create", ctypes.byref(h), arr, len(self.solvers))
+        self._h = h
+
+    @property
+    def launches_per_iter(self):
+        return int(load().ddfan_batch_launches_per_iter(self._h))
+
+    def iterate(self, n, use_graph=True, stream=None):
+        call("ddfan_batch_iterate", self._h, int(n), 1 if use_graph else 0, _stream(stream))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().ddfan_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

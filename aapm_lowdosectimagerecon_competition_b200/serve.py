@@ -292,11 +292,16 @@ class Engine:
 
 
 def latency_stats(finished, t0=None):
+    """Latency percentiles of finished requests: arrival to result (p50/p99),
+    and its two parts -- queueing (arrival to admission) and service
+    (admission to result, the reconstruction itself on a shared GPU)."""
     lat = np.array([f["t_done"] - f["t_arrival"] for f in finished]) if finished else np.zeros(0)
     qd = np.array([f["t_admit"] - f["t_arrival"] for f in finished]) if finished else np.zeros(0)
+    sv = np.array([f["t_done"] - f["t_admit"] for f in finished]) if finished else np.zeros(0)
     pct = lambda a, q: float(np.percentile(a, q)) if a.size else None
     return {"p50_s": pct(lat, 50), "p99_s": pct(lat, 99), "mean_s": float(lat.mean()) if lat.size else None,
-            "queue_p50_s": pct(qd, 50), "queue_p99_s": pct(qd, 99)}
+            "queue_p50_s": pct(qd, 50), "queue_p99_s": pct(qd, 99),
+            "service_p50_s": pct(sv, 50), "service_p99_s": pct(sv, 99), "completed": int(lat.size)}
 
 
 def run_batch(instances, engine):
@@ -317,6 +322,50 @@ def run_batch(instances, engine):
            "peak_gb": engine.peak_used / 1e9}
     out.update(latency_stats(fin))
     return out
+
+
+def run_batched(instances, device=0, sat="direct", back="adj"):
+    """All instances as one batch (device.OSSARTBatch): every solver is set up
+    and given its sinogram, then each batched iteration advances all of them
+    with one launch per kernel kind, subset step and tile class (one CUDA
+    graph); instances with fewer iterations are run in a second batch of the
+    rest.  Returns wall time (set-up, iterations and result copies included)
+    and the aggregate OS-SART iteration and sample rates."""
+    from .device import OSSARTBatch
+    dev = torch.device("cuda", device)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    solvers = []
+    for inst in instances:
+        s = inst.scan
+        x0, y0, xds, yds = dd2.fan_geometry(s.sid, s.sdd, s.DNU, s.detCellWidth, s.detCntIdx)
+        sv = OSSART(x0, y0, s.DNU, xds, yds, s.detCntIdx, s.hangs(), s.XN, s.YN, s.SLN, s.dx, mask=inst.mask,
+                    numOfOS=s.numOfOS, useFISTA=s.useFISTA, nonneg=s.nonneg, sat=sat, back=back,
+                    device=dev.index)
+        sv.set_sinogram(inst.proj_host)
+        sv.set_image(torch.zeros((s.YN, s.XN, s.SLN), device=dev))
+        solvers.append(sv)
+    t_setup = time.perf_counter() - t0
+    done = 0
+    remaining = list(range(len(instances)))
+    launches = 0
+    while remaining:
+        n = min(instances[i].iters for i in remaining) - done
+        b = OSSARTBatch([solvers[i] for i in remaining])
+        launches = max(launches, b.launches_per_iter)
+        b.iterate(n)
+        b.close()
+        done += n
+        remaining = [i for i in remaining if instances[i].iters > done]
+    images = [sv.image_host() for sv in solvers]
+    torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - t0
+    for sv in solvers:
+        sv.close()
+    iters = sum(inst.iters for inst in instances)
+    work = sum(inst.iters * inst.work for inst in instances)
+    return {"instances": len(instances), "wall_s": wall, "setup_s": t_setup, "iters_per_s": iters / wall,
+            "samples_per_s": work / wall, "launches_per_batched_iter": launches, "images": images}
 
 
 def plain_mex_seconds_per_iter(s, y_host, mask):

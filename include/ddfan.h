@@ -88,8 +88,11 @@ DDFAN_API int ddfan_fan_geometry(float sid, float sdd, int DNU, float detCellWid
  * the same 16 inputs in the same order, then the SAT precision and the output
  * buffer prj[PN][DNU][SLN] (the mex allocates it; here the caller does).
  * startIdx[nStartIdx] gives the first slice of each device's slab
- * (DD2MutiSlices.m:95-101); slabs run on devices 0..nStartIdx-1 in turn,
- * nStartIdx <= 0 or startIdx == NULL means one slab on the current device. */
+ * (DD2MutiSlices.m:95-101); slab k runs on device k mod (device count), each
+ * device's slabs on a host thread of its own so that devices work at the same
+ * time (as the reference's one std::thread per GPU, MultiSlicesProjGPU.cu:
+ * 474-484); nStartIdx <= 0 or startIdx == NULL means one slab on the current
+ * device. */
 DDFAN_API int ddfan_MultiSlicesProjGPU(float x0, float y0, int DNU, const float* xds,
                                        const float* yds, float imgXCenter, float imgYCenter,
                                        const float* hangs, int PN, int XN, int YN, int SLN,
@@ -213,6 +216,27 @@ DDFAN_API int ddfan_ossart_profile(ddfan_ossart* s, int numOfIter, void* stream,
                                    int* launches_by_kind);
 /* number of kernel launches one iteration issues */
 DDFAN_API int ddfan_ossart_launches_per_iter(const ddfan_ossart* s);
+
+/* ---- batched OS-SART: many reconstructions advanced together ----
+ * No counterpart in the reference, which runs one reconstruction per MATLAB
+ * call (AAPM_script/OSSART_AAPM.m:85, :92).  Groups n solvers created with
+ * DDFAN_SAT_DIRECT and one angle list for all slices (any sizes, subset
+ * counts, backprojectors; one device).  Each ddfan_batch_iterate iteration
+ * runs every solver's next OS-SART iteration with one launch per kernel
+ * kind, subset step and tile class over a device work list of all solvers'
+ * work items (view x channel block x slice tiles; voxel tiles x slice tiles),
+ * captured as one CUDA graph when use_graph != 0; each solver computes
+ * exactly what ddfan_ossart_iterate computes for it alone.  The batch does
+ * not own the solvers: they must outlive it, and their sinograms and images
+ * must be set (ordered before the iterate call's stream) first.  Results are
+ * read with ddfan_ossart_get_image. */
+typedef struct ddfan_batch_s ddfan_batch;
+
+DDFAN_API int ddfan_batch_create(ddfan_batch** out, ddfan_ossart* const* solvers, int n);
+DDFAN_API void ddfan_batch_destroy(ddfan_batch* b);
+DDFAN_API int ddfan_batch_iterate(ddfan_batch* b, int numOfIter, int use_graph, void* stream);
+/* kernel launches one batched iteration issues */
+DDFAN_API int ddfan_batch_launches_per_iter(const ddfan_batch* b);
 
 /* One-call host entry mirroring OSSART_AAPM(Proj, Views, initImg, conf,
  * numOfIter, numOfOS, mask, useFISTA) with the geometry already expanded. */

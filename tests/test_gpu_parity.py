@@ -139,8 +139,12 @@ def test_ref_mode_matches_reference_kernels(mods, name, c):
     assert rel(B, c["ref_back"]) < 2e-3
 
 
-def test_start_idx_slabs_match_single_slab(mods):
+@pytest.mark.parametrize("threads", ["device", "slab"])
+def test_start_idx_slabs_match_single_slab(mods, monkeypatch, threads):
+    """Slabs of startIdx equal the one-slab call; with threads=slab every slab
+    runs on a host thread of its own (concurrently, here on one GPU)."""
     dd2, configs, device, O = mods
+    monkeypatch.setenv("DDFAN_SLAB_THREADS", threads)
     g, vol, prj = make_case(configs, dd2, SLN=11, per_slice=True)
     one = fwd(dd2, g, vol, "hilo")
     args = (g["x0"], g["y0"], g["DNU"], g["xds"], g["yds"], g["cx"], g["cy"], g["h"], g["PN"], g["XN"],
