@@ -304,7 +304,8 @@ template <int ZL, int CG, int NZ>
 __global__ void __launch_bounds__(256, DDFAN_DD_FWD_MIN_CTAS) k_fwd_dd_batch(const DdFwdArgs* __restrict__ args,
                                                                               const int4* __restrict__ items) {
   const int4 it = items[blockIdx.x];
-  fwd_dd_body<ZL, CG, NZ>(args[it.x], it.y, it.z, it.w);
+  const DdFwdArgs a = args[it.x];  // a local copy: its fields stay in registers
+  fwd_dd_body<ZL, CG, NZ>(a, it.y, it.z, it.w);
 }
 
 // ============================================================ exact adjoint
@@ -495,7 +496,8 @@ template <int ZL, bool XM, int NZ>
 __global__ void __launch_bounds__(256, DDFAN_DD_BACK_MIN_CTAS) k_back_dd_batch(const DdAdjArgs* __restrict__ args,
                                                                                 const int4* __restrict__ items) {
   const int4 it = items[blockIdx.x];
-  back_dd_body<ZL, XM, NZ>(args[it.x], it.y, it.z);
+  const DdAdjArgs a = args[it.x];  // a local copy: its fields stay in registers
+  back_dd_body<ZL, XM, NZ>(a, it.y, it.z);
 }
 
 // ============================================================ reference backprojector
@@ -606,7 +608,8 @@ template <int ZL>
 __global__ void __launch_bounds__(256, DDFAN_REF_MIN_CTAS) k_back_ref_dd_batch(const DdRefArgs* __restrict__ args,
                                                                                 const int4* __restrict__ items) {
   const int4 it = items[blockIdx.x];
-  ref_dd_body<ZL>(args[it.x], it.y, it.z);
+  const DdRefArgs a = args[it.x];  // a local copy: its fields stay in registers
+  ref_dd_body<ZL>(a, it.y, it.z);
 }
 
 // ============================================================ staging

@@ -179,10 +179,16 @@ template <> struct AccS<SAT_FP64> {
 // 32-bit words of a cell's prefix sum
 template <int M> struct PsInfo { static constexpr int SW = M == SAT_FP32 ? 1 : 2; };
 
-// Correctly rounded reciprocal (IEEE round-to-nearest) of the footprint
-// length and of the bracket width: an approximate one moved row sums by ~1e-7
-// between kernels, which an OS-SART solve amplifies.
-__device__ __forceinline__ float rcp_exact(float x) { return __frcp_rn(x); }
+// Reciprocal of the footprint length and of the bracket width: the PTX
+// approximate reciprocal (at most 1 ulp from the correctly rounded one, per
+// the PTX ISA).  __frcp_rn in its place measured 30 % slower on the per-slice
+// c3 solve (3.09 -> 2.36 iterations/s); a 768-pixel-line test against the
+// FP64 oracle holds the 2e-6 bound with this one.
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 
 // ---------------------------------------------------------------- transposes
 
@@ -348,7 +354,7 @@ __global__ void __launch_bounds__(256) k_ps_fwd(PsFwdArgs a) {
       PhiS<M> cur;
       cur.load(line + i0, f);
       const PhiS<M> nxt = cur.down();
-      part = fmaf(nxt.diff(cur), rcp_exact(fmaf(fi, lF, lC)), part);
+      part = fmaf(nxt.diff(cur), rcp_approx(fmaf(fi, lF, lC)), part);
       cf += dcf;
       fi += 1.f;
       line += Nw;
@@ -445,7 +451,7 @@ __global__ void __launch_bounds__(256) k_ps_back_adj(PsBackArgs a) {
         f0 = line_at(b);
         c0 = fma(di, f0.x, f0.y);
       }
-      const float frac = fminf(fmaxf((float)(dk - c0) * rcp_exact((float)(c1 - c0)), 0.f), 1.f);
+      const float frac = fminf(fmaxf((float)(dk - c0) * rcp_approx((float)(c1 - c0)), 0.f), 1.f);
       PhiS<M> q;
       q.load(qrow + b, frac);
       return q;

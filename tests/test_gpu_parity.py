@@ -441,3 +441,29 @@ def test_slab_sharded_solve_matches_full(mods, monkeypatch, lists):
     assert [(a, b) for a, b, _ in parts] == [(0, 5), (5, 9)]
     joined = np.concatenate([img.cpu().numpy() for _, _, img in parts], axis=-1)
     assert rel(joined, whole.cpu().numpy()) < 1e-6
+
+
+@pytest.mark.parametrize("back", ["adj", "ref"])
+def test_slice_major_kernels_at_768_pixel_lines(mods, back):
+    """The slice-major kernels (taken by per-slice angle lists) at 768-pixel
+    lines, where the approximate reciprocal of the footprint length and of the
+    bracket width meets the longest lines: projection and backprojection
+    within the compensated 2e-6 bound of the FP64 oracle."""
+    dd2, configs, device, O = mods
+    s = configs.c2(SLN=3)
+    s.dx = 0.7 * 512 / 768
+    s.XN = s.YN = 768
+    PN = 48
+    x0, y0, xds, yds = dd2.fan_geometry(s.sid, s.sdd, s.DNU, s.detCellWidth, s.detCntIdx)
+    h = rebinned_angles(2304, 3, [0, 517, 1203])[:PN * 48:48].copy()
+    vol = configs.ellipsoid_phantom_3d(s)
+    rng = np.random.default_rng(4)
+    prj = rng.random((PN, s.DNU, s.SLN)).astype(np.float32)
+    got = dd2.MultiSlicesProjGPU(x0, y0, s.DNU, xds, yds, 0, 0, h, PN, s.XN, s.YN, s.SLN, vol, s.dx, sat="hilo")
+    exp = O.proj(x0, y0, s.DNU, xds, yds, 0, 0, h, PN, s.XN, s.YN, s.SLN, vol, s.dx)
+    assert rel(got, exp) < 2e-6
+    gb = dd2.MultiSlicesBackGPU(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0, 0, h, PN, s.XN, s.YN, s.SLN, prj, s.dx,
+                                sat="hilo", back=back)
+    eb = O.back(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0, 0, h, PN, s.XN, s.YN, s.SLN, prj, s.dx,
+                mode=O.ADJ if back == "adj" else O.REF)
+    assert rel(gb, eb) < 2e-6
