@@ -640,12 +640,14 @@ class ClockSampler:
 
 PROFILE_OF = {"fwd": "k_fwd_c3_subset.md", "back_a": "k_back_adj_c3_subset.md",
               "back_b": "k_back_adj_c3_subset.md"}
+PROFILE_OF_DIRECT = {"fwd": "k_fwd_dd_c3_subset.md", "back_a": "k_back_dd_c3_subset.md",
+                     "back_b": "k_back_dd_c3_subset.md"}
 
 
-def profiled_traffic(kernel):
+def profiled_traffic(kernel, sat="hilo"):
     """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
     recorded from an ncu capture of this kernel in profiles/, or None."""
-    name = PROFILE_OF.get(kernel)
+    name = (PROFILE_OF_DIRECT if sat == "direct" else PROFILE_OF).get(kernel)
     if not name:
         return None
     try:
@@ -756,7 +758,7 @@ def run_ours(args):
     achieved = alg[top] / (top_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": profiled_traffic(top), "algorithmic_bytes": alg[top],
+                "traffic": profiled_traffic(top, args.sat), "algorithmic_bytes": alg[top],
                 "launch_ms": top_ms,
                 "kernel_ms_per_iter": {k: round(v[0], 3) for k, v in prof.items()},
                 "note": "achieved = algorithmic bytes per launch / CUDA-event launch time; the "
