@@ -247,10 +247,12 @@ static int batch_create(Batch** out, Solver* const* solvers, int n) {
       const int fi = (int)fargs.size();
       fargs.push_back(fa);
       const int cw = fwd_cw(p.ZL, fnz), ncb = (s.U + cw - 1) / cw, nzg = (fa.nzt + fnz - 1) / fnz;
+      // z-tile groups outermost, as in the single-solve grid: the views in
+      // flight then share one group's slices, whose image part stays in L2
       auto& fl = fwd[{p.ZL, fnz}];
-      for (int row = 0; row < c; ++row)
-        for (int cb = 0; cb < ncb; ++cb)
-          for (int zg = 0; zg < nzg; ++zg) fl.push_back(make_int4(fi, row, cb, zg));
+      for (int zg = 0; zg < nzg; ++zg)
+        for (int row = 0; row < c; ++row)
+          for (int cb = 0; cb < ncb; ++cb) fl.push_back(make_int4(fi, row, cb, zg));
       BackEpi e{};
       e.out = s.d_x; e.xin = s.d_x; e.colsum = s.d_cols + (size_t)k * s.XN * s.YN;
       e.nonneg = s.nonneg; e.mask = p.has_mask ? p.d_mask : nullptr; e.zlo = 0; e.zhi = s.Zi;
@@ -271,10 +273,10 @@ static int batch_create(Batch** out, Solver* const* solvers, int n) {
         const int ty = ((s.YN + LT - 1) / LT) * ((s.XN + KT - 1) / KT);  // y rows as lines
         auto& lx = adjx[{p.ZL, bnz}];
         auto& ly = adjy[{p.ZL, bnz}];
-        for (int t = 0; t < tx; ++t)
-          for (int zg = 0; zg < nbz; ++zg) lx.push_back(make_int4(i1, t, zg, 0));
-        for (int t = 0; t < ty; ++t)
-          for (int zg = 0; zg < nbz; ++zg) ly.push_back(make_int4(i1 + 1, t, zg, 0));
+        for (int zg = 0; zg < nbz; ++zg)
+          for (int t = 0; t < tx; ++t) lx.push_back(make_int4(i1, t, zg, 0));
+        for (int zg = 0; zg < nbz; ++zg)
+          for (int t = 0; t < ty; ++t) ly.push_back(make_int4(i1 + 1, t, zg, 0));
       } else {
         int LT, KT;
         ref_tile(p.ZL, &LT, &KT);
@@ -282,8 +284,8 @@ static int batch_create(Batch** out, Solver* const* solvers, int n) {
         rargs.push_back(ar);
         const int tiles = ((s.YN + LT - 1) / LT) * ((s.XN + KT - 1) / KT);
         auto& lr = ref[{p.ZL, 1}];
-        for (int t = 0; t < tiles; ++t)
-          for (int zt = 0; zt < nzt; ++zt) lr.push_back(make_int4(ri, t, zt, 0));
+        for (int zt = 0; zt < nzt; ++zt)
+          for (int t = 0; t < tiles; ++t) lr.push_back(make_int4(ri, t, zt, 0));
       }
     }
     auto emit = [&](int kind, std::map<std::pair<int, int>, std::vector<int4>>& m) {
