@@ -624,14 +624,15 @@ int launch_publish_masked(const float* x, int Zi, const float* x0, int Z, const 
 template <int ZL>
 static void fwd_dd_go(const DdFwdArgs& a, int nzt, cudaStream_t st) {
   constexpr int CG = DdFwdCG<ZL>::v;
-  constexpr int kMaxRows = 65535;  // grid y limit
+  constexpr int kMaxRows = DDFAN_DD_FWD_ROWS_X ? (1 << 30) : 65535;  // grid x / y limit
   const auto go = [&](auto nz) {
     constexpr int NZ = decltype(nz)::value;
     using T = DdFwdTile<ZL, CG, NZ>;
     for (int r0 = 0; r0 < a.PN; r0 += kMaxRows) {
       DdFwdArgs b = a;
       b.row0 = r0;
-      dim3 grid((a.U + T::CW - 1) / T::CW, std::min(a.PN - r0, kMaxRows), (nzt + NZ - 1) / NZ);
+      const int rows = std::min(a.PN - r0, kMaxRows), cblk = (a.U + T::CW - 1) / T::CW;
+      const dim3 grid(DDFAN_DD_FWD_ROWS_X ? rows : cblk, DDFAN_DD_FWD_ROWS_X ? cblk : rows, (nzt + NZ - 1) / NZ);
       k_fwd_dd<ZL, CG, NZ><<<grid, T::NT, 0, st>>>(b);
     }
   };
@@ -698,9 +699,13 @@ static void back_dd_zl(int ZL, const DdAdjArgs& a, int nzt, cudaStream_t st) {
 
 template <int ZL>
 static void ref_dd_go(const DdRefArgs& a, int nzt, cudaStream_t st) {
-  using T = BackTile<ZL>;
+  using T = DdBackTile<ZL>;
   const int tiles = ((a.YN + T::LT - 1) / T::LT) * ((a.XN + T::KT - 1) / T::KT);
-  k_back_ref_dd<ZL><<<dim3(tiles, 1, nzt), T::NT, 0, st>>>(a);
+  switch (dd_nz(nzt)) {
+    case 4: k_back_ref_dd<ZL, 4><<<dim3(tiles, 1, (nzt + 3) / 4), T::NT, 0, st>>>(a); break;
+    case 2: k_back_ref_dd<ZL, 2><<<dim3(tiles, 1, (nzt + 1) / 2), T::NT, 0, st>>>(a); break;
+    default: k_back_ref_dd<ZL, 1><<<dim3(tiles, 1, nzt), T::NT, 0, st>>>(a); break;
+  }
 }
 
 int make_back_dd_args(const Plan& p, int back_mode, const float* w, const ViewGeom* vg, const double2* fc,
@@ -716,6 +721,7 @@ int make_back_dd_args(const Plan& p, int back_mode, const float* w, const ViewGe
     a.inv_sid = p.inv_sid; a.inv_dbeta = p.inv_dbeta; a.cnt = (double)p.detCntIdx + 0.5;
     a.epi = epi;
     a.zt0 = zt0;
+    a.nzt = nzt;
     *ref = a;
     return nzt;
   }

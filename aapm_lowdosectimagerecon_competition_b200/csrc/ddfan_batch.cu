@@ -68,15 +68,6 @@ void adj_tile(int ZL, int* LT, int* KT) {
   }
 }
 
-void ref_tile(int ZL, int* LT, int* KT) {
-  switch (ZL) {
-    case 8: *LT = BackTile<8>::LT; *KT = BackTile<8>::KT; break;
-    case 4: *LT = BackTile<4>::LT; *KT = BackTile<4>::KT; break;
-    case 2: *LT = BackTile<2>::LT; *KT = BackTile<2>::KT; break;
-    default: *LT = BackTile<1>::LT; *KT = BackTile<1>::KT; break;
-  }
-}
-
 template <int ZL, int NZ>
 void go_fwd(const DdFwdArgs* a, const int4* it, unsigned n, cudaStream_t st) {
   k_fwd_dd_batch<ZL, DdFwdCG<ZL>::v, NZ><<<n, 256, 0, st>>>(a, it);
@@ -88,9 +79,9 @@ void go_adj(bool xm, const DdAdjArgs* a, const int4* it, unsigned n, cudaStream_
   else k_back_dd_batch<ZL, false, NZ><<<n, 256, 0, st>>>(a, it);
 }
 
-template <int ZL>
+template <int ZL, int NZ>
 void go_ref(const DdRefArgs* a, const int4* it, unsigned n, cudaStream_t st) {
-  k_back_ref_dd_batch<ZL><<<n, 256, 0, st>>>(a, it);
+  k_back_ref_dd_batch<ZL, NZ><<<n, 256, 0, st>>>(a, it);
 }
 
 #define DDFAN_BATCH_ZL_NZ(ZLv, NZv, CALL) \
@@ -179,12 +170,20 @@ static int batch_iteration(Batch& b, cudaStream_t st) {
       } while (0);
     } else {
       ProfScope ps(KIND_BACK_A, st);
-      switch (L.ZL) {
-        case 8: go_ref<8>(b.d_rargs, it, n, st); break;
-        case 4: go_ref<4>(b.d_rargs, it, n, st); break;
-        case 2: go_ref<2>(b.d_rargs, it, n, st); break;
-        default: go_ref<1>(b.d_rargs, it, n, st); break;
-      }
+      do {
+        DDFAN_BATCH_ZL_NZ(8, 4, (go_ref<8, 4>(b.d_rargs, it, n, st)))
+        DDFAN_BATCH_ZL_NZ(8, 2, (go_ref<8, 2>(b.d_rargs, it, n, st)))
+        DDFAN_BATCH_ZL_NZ(8, 1, (go_ref<8, 1>(b.d_rargs, it, n, st)))
+        DDFAN_BATCH_ZL_NZ(4, 4, (go_ref<4, 4>(b.d_rargs, it, n, st)))
+        DDFAN_BATCH_ZL_NZ(4, 2, (go_ref<4, 2>(b.d_rargs, it, n, st)))
+        DDFAN_BATCH_ZL_NZ(4, 1, (go_ref<4, 1>(b.d_rargs, it, n, st)))
+        DDFAN_BATCH_ZL_NZ(2, 4, (go_ref<2, 4>(b.d_rargs, it, n, st)))
+        DDFAN_BATCH_ZL_NZ(2, 2, (go_ref<2, 2>(b.d_rargs, it, n, st)))
+        DDFAN_BATCH_ZL_NZ(2, 1, (go_ref<2, 1>(b.d_rargs, it, n, st)))
+        DDFAN_BATCH_ZL_NZ(1, 4, (go_ref<1, 4>(b.d_rargs, it, n, st)))
+        DDFAN_BATCH_ZL_NZ(1, 2, (go_ref<1, 2>(b.d_rargs, it, n, st)))
+        DDFAN_BATCH_ZL_NZ(1, 1, (go_ref<1, 1>(b.d_rargs, it, n, st)))
+      } while (0);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "batched launch (kind %d): %s", L.kind, cudaGetErrorString(e));
@@ -247,12 +246,19 @@ static int batch_create(Batch** out, Solver* const* solvers, int n) {
       const int fi = (int)fargs.size();
       fargs.push_back(fa);
       const int cw = fwd_cw(p.ZL, fnz), ncb = (s.U + cw - 1) / cw, nzg = (fa.nzt + fnz - 1) / fnz;
-      // z-tile groups outermost, as in the single-solve grid: the views in
-      // flight then share one group's slices, whose image part stays in L2
+      // z-tile groups outermost and the rest in the single-solve grid's
+      // order: the CTAs in flight share one group's slices, whose image part
+      // then stays in L2
       auto& fl = fwd[{p.ZL, fnz}];
-      for (int zg = 0; zg < nzg; ++zg)
-        for (int row = 0; row < c; ++row)
-          for (int cb = 0; cb < ncb; ++cb) fl.push_back(make_int4(fi, row, cb, zg));
+      for (int zg = 0; zg < nzg; ++zg) {
+        if (DDFAN_DD_FWD_ROWS_X) {
+          for (int cb = 0; cb < ncb; ++cb)
+            for (int row = 0; row < c; ++row) fl.push_back(make_int4(fi, row, cb, zg));
+        } else {
+          for (int row = 0; row < c; ++row)
+            for (int cb = 0; cb < ncb; ++cb) fl.push_back(make_int4(fi, row, cb, zg));
+        }
+      }
       BackEpi e{};
       e.out = s.d_x; e.xin = s.d_x; e.colsum = s.d_cols + (size_t)k * s.XN * s.YN;
       e.nonneg = s.nonneg; e.mask = p.has_mask ? p.d_mask : nullptr; e.zlo = 0; e.zhi = s.Zi;
@@ -278,14 +284,15 @@ static int batch_create(Batch** out, Solver* const* solvers, int n) {
         for (int zg = 0; zg < nbz; ++zg)
           for (int t = 0; t < ty; ++t) ly.push_back(make_int4(i1 + 1, t, zg, 0));
       } else {
+        const int bnz = dd_nz(nzt), nbz = (nzt + bnz - 1) / bnz;
         int LT, KT;
-        ref_tile(p.ZL, &LT, &KT);
+        adj_tile(p.ZL, &LT, &KT);  // the REF kernel uses the exact adjoint's voxel tile
         const int ri = (int)rargs.size();
         rargs.push_back(ar);
         const int tiles = ((s.YN + LT - 1) / LT) * ((s.XN + KT - 1) / KT);
-        auto& lr = ref[{p.ZL, 1}];
-        for (int zt = 0; zt < nzt; ++zt)
-          for (int t = 0; t < tiles; ++t) lr.push_back(make_int4(ri, t, zt, 0));
+        auto& lr = ref[{p.ZL, bnz}];
+        for (int zg = 0; zg < nbz; ++zg)
+          for (int t = 0; t < tiles; ++t) lr.push_back(make_int4(ri, t, zg, 0));
       }
     }
     auto emit = [&](int kind, std::map<std::pair<int, int>, std::vector<int4>>& m) {

@@ -38,11 +38,33 @@ namespace ddfan {
 #define DDFAN_DD_BACK_MIN_CTAS 2
 #endif
 
+// a += w v on 4 slices, as two packed fma.rn.f32x2 (sm_100: two lanes of
+// round-to-nearest FMA per instruction, the same results as four fmaf; half
+// the FMA instructions took a c3 subset's forward from 2.50 to 2.41 ms).
+// DDFAN_FFMA2=0 builds the scalar form.
+#ifndef DDFAN_FFMA2
+#define DDFAN_FFMA2 1
+#endif
+__device__ __forceinline__ void fma2(float& a0, float& a1, float w, float v0, float v1) {
+  asm("{\n\t.reg .b64 ra, rv, rw;\n\t"
+      "mov.b64 ra, {%0, %1};\n\t"
+      "mov.b64 rv, {%2, %3};\n\t"
+      "mov.b64 rw, {%4, %4};\n\t"
+      "fma.rn.f32x2 ra, rw, rv, ra;\n\t"
+      "mov.b64 {%0, %1}, ra;\n\t}"
+      : "+f"(a0), "+f"(a1)
+      : "f"(v0), "f"(v1), "f"(w));
+}
 __device__ __forceinline__ void fma4(float (&a)[4], float w, const float4& v) {
+#if DDFAN_FFMA2
+  fma2(a[0], a[1], w, v.x, v.y);
+  fma2(a[2], a[3], w, v.z, v.w);
+#else
   a[0] = fmaf(w, v.x, a[0]);
   a[1] = fmaf(w, v.y, a[1]);
   a[2] = fmaf(w, v.z, a[2]);
   a[3] = fmaf(w, v.w, a[3]);
+#endif
 }
 
 // The walk from (k0, f0) to (k1, f1) as three weights: w0 on the value at
@@ -292,10 +314,23 @@ __device__ __forceinline__ void fwd_dd_body(const DdFwdArgs& a, int row, int cbl
   }
 }
 
+// Grid order of the forward: with DDFAN_DD_FWD_ROWS_X the view rows run
+// along grid x (dispatched first), so the CTAs in flight are every view of a
+// few channel blocks -- rays at one distance from the centre, whose image
+// footprint is an annulus -- instead of every channel block of a few views,
+// which spans the whole image.
+#ifndef DDFAN_DD_FWD_ROWS_X
+#define DDFAN_DD_FWD_ROWS_X 0
+#endif
+
 // One CTA per (view row, channel block, z-tile group) of one call.
 template <int ZL, int CG, int NZ>
 __global__ void __launch_bounds__(256, DDFAN_DD_FWD_MIN_CTAS) k_fwd_dd(const __grid_constant__ DdFwdArgs a) {
+#if DDFAN_DD_FWD_ROWS_X
+  fwd_dd_body<ZL, CG, NZ>(a, a.row0 + (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z);
+#else
   fwd_dd_body<ZL, CG, NZ>(a, a.row0 + (int)blockIdx.y, (int)blockIdx.x, (int)blockIdx.z);
+#endif
 }
 
 // One launch over a work list of many calls (batched reconstructions): CTA
@@ -509,51 +544,66 @@ struct DdRefArgs {
   int PN, U, Z, XN, YN;
   double ocx, ocy, dx, inv_sid, inv_dbeta, cnt;  // cnt = detCntIdx + 1 - 0.5
   BackEpi epi;
-  int zt0;
+  int zt0, nzt;
 };
 
 // The reference backprojector's formula (AAPM_script/MultiSlicesBackGPU.cu:
-// 115-184), geometry as in k_back_ref (FP64, once per voxel and view of the
-// tile); the difference of the two channel prefix-sum samples is walked over
-// the residual itself.
-template <int ZL>
-__device__ __forceinline__ void ref_dd_body(const DdRefArgs& a, int tile, int ztg) {
-  using T = BackTile<ZL>;
-  constexpr int NT = T::NT, VG = T::VG, SPL = T::SPL, KT = T::KT, LT = T::LT, NV = T::NV;
-  constexpr int VC = (2048 / NV) < 1 ? 1 : ((2048 / NV) > 4 ? 4 : 2048 / NV);
-  __shared__ int2 s_i[VC][NV];
-  __shared__ float2 s_f[VC][NV];
-  __shared__ float s_w[VC][NV];
-  __shared__ int s_p[VC];
-  const int tid = threadIdx.x;
-  const int zl = tid % ZL, g = tid / ZL;
-  const int zt = ztg + a.zt0;
-  const int zb = zt * ZL + zl;
+// 115-184): angular detector coordinate alpha = asin(cross / (|s| l)),
+// footprint half-width dx ddv / (2 l^2), weight dx l / ddv, coordinate
+// alpha / dbeta + detCntIdx + 1, evaluated in FP64 once per (voxel, view) of
+// a warp's voxels; the difference of the two channel prefix-sum samples is
+// walked over the residual itself.  Voxel tile as the exact adjoint's (lines
+// are image rows, k = x), VG voxels x NZ z-tiles per thread, ZL views per
+// warp chunk, per-warp synchronisation only.
+template <int ZL, int NZ>
+__device__ __forceinline__ void ref_dd_body(const DdRefArgs& a, int tile, int zgrp) {
+  using T = DdBackTile<ZL>;
+  constexpr int NT = T::NT, VG = T::VG, SPL = T::SPL, KT = T::KT, LT = T::LT;
+  constexpr int NW = NT / 32, GW = 32 / ZL;
+  constexpr int VCW = ZL;  // views per warp chunk
+  __shared__ int2 s_i[NW][VCW][GW][VG];
+  __shared__ float2 s_f[NW][VCW][GW][VG];
+  __shared__ float s_w[NW][VCW][GW][VG];
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  const int zl = lane % ZL, gw = lane / ZL;
+  const int zt_first = a.zt0 + zgrp * NZ;
+  int zbk[NZ], zoff[NZ];
+  bool zok[NZ];
+#pragma unroll
+  for (int z = 0; z < NZ; ++z) {
+    zbk[z] = (zt_first + z) * ZL + zl;
+    zok[z] = zgrp * NZ + z < a.nzt && zbk[z] < a.P4;
+    zoff[z] = zok[z] ? z * ZL : 0;  // a tile past the image reads the first one again (dropped)
+  }
   const int ntx = (a.XN + KT - 1) / KT;
   const int ty = tile / ntx, tx = tile - ty * ntx;
   const int y0 = ty * LT, x0 = tx * KT;
+  const int g = w * GW + gw;
   const int l = g / SPL, sg = g - l * SPL;
   const int iy = y0 + l, ixs = x0 + sg * VG;
-  const bool active = zb < a.P4 && iy < a.YN && ixs < a.XN;
-  float acc[VG][4];
-  float4 vm[1] = {make_float4(0.f, 0.f, 0.f, 0.f)};  // first interior value (see walk_nz)
+  const bool active = zok[0] && iy < a.YN && ixs < a.XN;
+  float acc[VG][NZ][4];
+  float4 vm[NZ];  // first interior values (kept between walks; see walk_nz)
 #pragma unroll
-  for (int v = 0; v < VG; ++v) acc[v][0] = acc[v][1] = acc[v][2] = acc[v][3] = 0.f;
+  for (int z = 0; z < NZ; ++z) vm[z] = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+  for (int v = 0; v < VG; ++v)
+#pragma unroll
+    for (int z = 0; z < NZ; ++z) acc[v][z][0] = acc[v][z][1] = acc[v][z][2] = acc[v][z][3] = 0.f;
   const double Ud = (double)a.U;
   const size_t P4 = (size_t)a.P4;
   const size_t vstride = (size_t)(a.U + 1) * P4;
-  for (int v0 = 0; v0 < a.PN; v0 += VC) {
-    const int nvc = min(VC, a.PN - v0);
-    if (tid < VC) s_p[tid] = v0 + tid;
-    for (int e = tid; e < VC * NV; e += NT) {
-      const int vv = e / NV, r = e - vv * NV;
-      const int ly = r / KT, lx = r - ly * KT;
-      const int yy = y0 + ly, xx = x0 + lx;
+  for (int v0 = 0; v0 < a.PN; v0 += VCW) {
+    const int nvc = min(VCW, a.PN - v0);
+    for (int e = lane; e < VCW * GW * VG; e += 32) {
+      const int vv = e / (GW * VG), r = e - vv * (GW * VG);
+      const int gl = r / VG, v = r - gl * VG;
+      const int gg = w * GW + gl;
+      const int yy = y0 + gg / SPL, xx = x0 + (gg % SPL) * VG + v;
       int2 ii = make_int2(0, 0);
       float2 ff = make_float2(0.f, 0.f);
-      float w = 0.f;
-      if (vv < nvc && yy < a.YN && xx < a.XN &&
-          (!a.epi.mask || a.epi.mask[(size_t)yy * a.XN + xx] != 0)) {
+      float wt = 0.f;
+      if (vv < nvc && yy < a.YN && xx < a.XN && (!a.epi.mask || a.epi.mask[(size_t)yy * a.XN + xx] != 0)) {
         const ViewGeom& G = a.vg[v0 + vv];
         const double sx = G.sx, sy = G.sy;
         const double ddx = (xx - a.ocx) * a.dx - sx, ddy = (yy - a.ocy) * a.dx - sy;
@@ -562,54 +612,58 @@ __device__ __forceinline__ void ref_dd_body(const DdRefArgs& a, int tile, int zt
         const double alpha = asin((sy * ddx - sx * ddy) * a.inv_sid / ln);
         const double ddv = fabs(sx) > fabs(sy) ? ddx : ddy;
         const double da = ddv / l2 * a.dx * 0.5;
-        w = (float)(a.dx / ddv * ln);
+        wt = (float)(a.dx / ddv * ln);
         const double cL = fmin(fmax((alpha - da) * a.inv_dbeta + a.cnt, 0.0), Ud);
         const double cR = fmin(fmax((alpha + da) * a.inv_dbeta + a.cnt, 0.0), Ud);
         ii = make_int2(min((int)cL, a.U - 1), min((int)cR, a.U - 1));
         ff = make_float2((float)(cL - ii.x), (float)(cR - ii.y));
       }
-      s_i[vv][r] = ii;
-      s_f[vv][r] = ff;
-      s_w[vv][r] = w;
+      s_i[w][vv][gl][v] = ii;
+      s_f[w][vv][gl][v] = ff;
+      s_w[w][vv][gl][v] = wt;
     }
-    __syncthreads();
+    __syncwarp();
     if (active) {
       for (int vv = 0; vv < nvc; ++vv) {
-        const float4* base = a.q + (size_t)s_p[vv] * vstride + zb;
+        const float4* base = a.q + (size_t)(v0 + vv) * vstride + zbk[0];
 #pragma unroll
         for (int v = 0; v < VG; ++v) {
-          const int r = l * KT + sg * VG + v;
-          const int2 ii = s_i[vv][r];
-          const float2 ff = s_f[vv][r];
-          const float3 wt = walk3(ii.x, ff.x, ii.y, ff.y, s_w[vv][r]);
-          float4 cur[1] = {__ldg(base + (size_t)ii.x * P4)};
-          const int zo[1] = {0};
-          walk_nz<1>(reinterpret_cast<float(&)[1][4]>(acc[v]), cur, vm, base, P4, zo, ii.x, ii.y, a.U,
-                     make_float4(wt.x, wt.y, wt.z, 0.f));
+          const int2 ii = s_i[w][vv][gw][v];
+          const float2 ff = s_f[w][vv][gw][v];
+          const float3 wt = walk3(ii.x, ff.x, ii.y, ff.y, s_w[w][vv][gw][v]);
+          float4 cur[NZ];
+          const float4* p0 = base + (size_t)ii.x * P4;
+#pragma unroll
+          for (int z = 0; z < NZ; ++z) cur[z] = __ldg(p0 + zoff[z]);
+          walk_nz<NZ>(acc[v], cur, vm, base, P4, zoff, ii.x, ii.y, a.U, make_float4(wt.x, wt.y, wt.z, 0.f));
         }
       }
     }
-    __syncthreads();
+    __syncwarp();
   }
   if (!active) return;
 #pragma unroll
-  for (int v = 0; v < VG; ++v)
-    if (ixs + v < a.XN) back_store(a.epi, ixs + v, iy, zb, a.XN, a.Z, false, acc[v]);
+  for (int v = 0; v < VG; ++v) {
+    if (ixs + v >= a.XN) break;
+#pragma unroll
+    for (int z = 0; z < NZ; ++z)
+      if (zok[z]) back_store(a.epi, ixs + v, iy, zbk[z], a.XN, a.Z, false, acc[v][z]);
+  }
 }
 
-// One CTA per (voxel tile, z-tile) of one call.
-template <int ZL>
-__global__ void __launch_bounds__(256, DDFAN_REF_MIN_CTAS) k_back_ref_dd(const __grid_constant__ DdRefArgs a) {
-  ref_dd_body<ZL>(a, (int)blockIdx.x, (int)blockIdx.z);
+// One CTA per (voxel tile, z-tile group) of one call.
+template <int ZL, int NZ>
+__global__ void __launch_bounds__(256, DDFAN_DD_BACK_MIN_CTAS) k_back_ref_dd(const __grid_constant__ DdRefArgs a) {
+  ref_dd_body<ZL, NZ>(a, (int)blockIdx.x, (int)blockIdx.z);
 }
 
-// The work-list launch: CTA b takes item {call, voxel tile, z-tile} = items[b].
-template <int ZL>
-__global__ void __launch_bounds__(256, DDFAN_REF_MIN_CTAS) k_back_ref_dd_batch(const DdRefArgs* __restrict__ args,
-                                                                                const int4* __restrict__ items) {
+// The work-list launch: CTA b takes item {call, voxel tile, z-tile group} = items[b].
+template <int ZL, int NZ>
+__global__ void __launch_bounds__(256, DDFAN_DD_BACK_MIN_CTAS) k_back_ref_dd_batch(const DdRefArgs* __restrict__ args,
+                                                                                    const int4* __restrict__ items) {
   const int4 it = items[blockIdx.x];
   const DdRefArgs a = args[it.x];  // a local copy: its fields stay in registers
-  ref_dd_body<ZL>(a, it.y, it.z);
+  ref_dd_body<ZL, NZ>(a, it.y, it.z);
 }
 
 // ============================================================ staging

@@ -3,7 +3,8 @@
 Workload (one GPU, or one independent instance per rank): 512 x 512 x 128
 slices at 0.7 mm, 2304 views over 360 deg, 736 arc channels at 1.2858 mm,
 sid 595 mm, sdd 1085.6 mm, 24 ordered subsets, FISTA momentum and
-non-negativity, exact-adjoint backprojector, the direct mode (every
+non-negativity, the reference's backprojector (the one OSSART_AAPM.m
+drives; --back adj selects the exact adjoint), the direct mode (every
 prefix-sum difference summed from the values it telescopes to; --sat fp32 /
 hilo / fp64 selects prefix-sum tables instead);
 the sinogram is the log of seeded Poisson counts at I0 = 1.5e5 photons/ray of
@@ -42,7 +43,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--sat", default="direct", choices=["fp32", "hilo", "fp64", "direct"])
-    ap.add_argument("--back", default="adj", choices=["ref", "adj"])
+    ap.add_argument("--back", default="ref", choices=["ref", "adj"])
     ap.add_argument("--slices", type=int, default=128)
     ap.add_argument("--subsets", type=int, default=24, help="c3: ordered subsets (the configuration has 24)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -541,7 +542,7 @@ def config_dict(s, args, n):
 
 # ----------------------------------------------------------------- CPU port
 
-def cpu_port_timing(s, slices, iters=1, nthreads=None):
+def cpu_port_timing(s, slices, iters=1, nthreads=None, back="ref"):
     """Seconds per OS-SART iteration of the FP64 CPU port on `slices` slices."""
     from oracle import oracle as O
     from oracle import np_oracle as N
@@ -552,7 +553,7 @@ def cpu_port_timing(s, slices, iters=1, nthreads=None):
     nt = nthreads or (os.cpu_count() or 1)
     _, secs = O.ossart(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0.0, 0.0, h, s.PN, s.XN, s.YN, slices,
                        y, init, s.dx, None, iters, s.numOfOS, s.useFISTA, s.nonneg,
-                       back_mode=O.ADJ, nthreads=nt, timing=True)
+                       back_mode=O.ADJ if back == "adj" else O.REF, nthreads=nt, timing=True)
     return secs / iters, nt
 
 
@@ -567,11 +568,11 @@ def run_reference(args):
     from oracle import oracle as O
     O.build()
     for _ in range(max(0, min(args.warmup, 1))):
-        cpu_port_timing(s, 1, 1)
+        cpu_port_timing(s, 1, 1, back=args.back)
     per = []
     nt = 1
     for _ in range(args.steps):
-        sec, nt = cpu_port_timing(s, sample, 1)
+        sec, nt = cpu_port_timing(s, sample, 1, back=args.back)
         per.append(sec * s.SLN / sample)
     t = statistics.mean(per)
     v = 1.0 / t
@@ -638,16 +639,21 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-PROFILE_OF = {"fwd": "k_fwd_c3_subset.md", "back_a": "k_back_adj_c3_subset.md",
-              "back_b": "k_back_adj_c3_subset.md"}
-PROFILE_OF_DIRECT = {"fwd": "k_fwd_dd_c3_subset.md", "back_a": "k_back_dd_c3_subset.md",
-                     "back_b": "k_back_dd_c3_subset.md"}
+# ncu summaries in profiles/ by (direct mode?, backprojector) and kernel slot
+PROFILE_OF = {
+    (False, "adj"): {"fwd": "k_fwd_c3_subset.md", "back_a": "k_back_adj_c3_subset.md",
+                     "back_b": "k_back_adj_c3_subset.md"},
+    (False, "ref"): {"fwd": "k_fwd_c3_subset.md"},
+    (True, "adj"): {"fwd": "k_fwd_dd_c3_subset.md", "back_a": "k_back_dd_c3_subset.md",
+                    "back_b": "k_back_dd_c3_subset.md"},
+    (True, "ref"): {"fwd": "k_fwd_dd_c3_subset.md", "back_a": "k_back_ref_dd_c3_subset.md"},
+}
 
 
-def profiled_traffic(kernel, sat="hilo"):
+def profiled_traffic(kernel, sat="hilo", back="adj"):
     """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
     recorded from an ncu capture of this kernel in profiles/, or None."""
-    name = (PROFILE_OF_DIRECT if sat == "direct" else PROFILE_OF).get(kernel)
+    name = PROFILE_OF[(sat == "direct", back)].get(kernel)
     if not name:
         return None
     try:
@@ -758,7 +764,7 @@ def run_ours(args):
     achieved = alg[top] / (top_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": profiled_traffic(top, args.sat), "algorithmic_bytes": alg[top],
+                "traffic": profiled_traffic(top, args.sat, args.back), "algorithmic_bytes": alg[top],
                 "launch_ms": top_ms,
                 "kernel_ms_per_iter": {k: round(v[0], 3) for k, v in prof.items()},
                 "note": "achieved = algorithmic bytes per launch / CUDA-event launch time; the "

@@ -65,6 +65,9 @@ CASES = {
     "single_slice": dict(SLN=1),
     "odd_slices": dict(SLN=13, XN=24, YN=30),
     "many_slices": dict(SLN=64, XN=32, YN=32, PN=30),
+    # 46 float4 slice blocks: two groups of 4 z-tiles of 8 blocks, the second
+    # holding 1.75 tiles (partial group and partial tile in the direct kernels)
+    "deep_partial_zgroups": dict(SLN=181, XN=20, YN=18, PN=24, masked=True),
 }
 
 
