@@ -27,6 +27,8 @@ SIGNATURES = {
     "ddfan_version": (_i, []),
     "ddfan_tune_set_zl": (_i, [_i, _i]),
     "ddfan_tune_get_zl": (_i, [_i]),
+    "ddfan_tune_set_nz": (_i, [_i, _i]),
+    "ddfan_tune_get_nz": (_i, [_i]),
     "ddfan_plan_estimate_bytes": (_sz, [_i, _i, _i, _i, _i, _i]),
     "ddfan_ossart_estimate_bytes": (_sz, [_i, _i, _i, _i, _i, _i, _i]),
     "ddfan_fan_geometry": (_i, [_f, _f, _i, _f, _f, _p, _p, _p, _p]),

@@ -71,6 +71,7 @@ LaunchProfiler::~LaunchProfiler() {
 // number of 4-slice blocks; consulted before the built-in cost model.
 static std::mutex g_tune_mutex;
 static std::map<int, int> g_tuned_zl;
+static std::map<int, int> g_tuned_nz;  // z-tiles per thread of the direct kernels
 
 static int tuned_zl(int ZB) {
   std::lock_guard<std::mutex> lock(g_tune_mutex);
@@ -98,6 +99,12 @@ int pow2_zl(int ZB) {
     if (c < bc) { bc = c; best = w; }
   }
   return best;
+}
+
+int plan_nz(int ZB) {
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  auto it = g_tuned_nz.find(ZB);
+  return it == g_tuned_nz.end() ? DDFAN_DD_NZ : it->second;
 }
 
 int plan_zl(int ZB, int zl_force) {
@@ -243,7 +250,7 @@ int plan_create(Plan** out, const PlanDesc& d) {
   Plan& p = *P;
   p.device = d.device;
   p.XN = d.XN; p.YN = d.YN; p.U = d.DNU; p.Z = d.SLN; p.ZB = (d.SLN + 3) / 4;
-  p.PNmax = d.PNmax; p.mode = d.sat_mode; p.ZL = plan_zl(p.ZB, d.zl_force);
+  p.PNmax = d.PNmax; p.mode = d.sat_mode; p.ZL = plan_zl(p.ZB, d.zl_force); p.NZ = plan_nz(p.ZB);
   p.P4 = p.ZB;
   // whole z-tiles: the padding blocks of the last tile are never written; the
   // projectors read them only for the slices past Z, whose results they drop
@@ -636,7 +643,7 @@ static void fwd_dd_go(const DdFwdArgs& a, int nzt, cudaStream_t st) {
       k_fwd_dd<ZL, CG, NZ><<<grid, T::NT, 0, st>>>(b);
     }
   };
-  switch (dd_nz(nzt)) {
+  switch (dd_nz(nzt, a.nzc)) {
     case 4: go(std::integral_constant<int, 4>()); break;
     case 2: go(std::integral_constant<int, 2>()); break;
     default: go(std::integral_constant<int, 1>()); break;
@@ -651,7 +658,7 @@ DdFwdArgs make_fwd_dd_args(const Plan& p, const float* img, const ViewGeom* vg, 
   a.vg = vg; a.fc = fc; a.cvd = cvd; a.order = order;
   a.out = out; a.orow = orow; a.ostride = ostride;
   a.PN = PN; a.U = p.U; a.Z = p.Z; a.XN = p.XN; a.YN = p.YN; a.dx = (float)p.dx;
-  a.zlo = zlo; a.zhi = zhi < 0 ? p.Z : zhi; a.row0 = 0;
+  a.zlo = zlo; a.zhi = zhi < 0 ? p.Z : zhi; a.row0 = 0; a.nzc = p.NZ;
   if (res) {
     a.y = res->y; a.yview = res->yview; a.rowsum = res->rowsum; a.wgt = res->wgt; a.ystride = res->ystride;
   }
@@ -680,7 +687,7 @@ static void back_dd_go(const DdAdjArgs& a, int nzt, cudaStream_t st) {
   using T = DdBackTile<ZL>;
   const int nl = XM ? a.XN : a.YN, N = XM ? a.YN : a.XN;
   const int tiles = ((nl + T::LT - 1) / T::LT) * ((N + T::KT - 1) / T::KT);
-  switch (dd_nz(nzt)) {
+  switch (dd_nz(nzt, a.nzc)) {
     case 4: k_back_dd<ZL, XM, 4><<<dim3(tiles, 1, (nzt + 3) / 4), T::NT, 0, st>>>(a); break;
     case 2: k_back_dd<ZL, XM, 2><<<dim3(tiles, 1, (nzt + 1) / 2), T::NT, 0, st>>>(a); break;
     default: k_back_dd<ZL, XM, 1><<<dim3(tiles, 1, nzt), T::NT, 0, st>>>(a); break;
@@ -701,7 +708,7 @@ template <int ZL>
 static void ref_dd_go(const DdRefArgs& a, int nzt, cudaStream_t st) {
   using T = DdBackTile<ZL>;
   const int tiles = ((a.YN + T::LT - 1) / T::LT) * ((a.XN + T::KT - 1) / T::KT);
-  switch (dd_nz(nzt)) {
+  switch (dd_nz(nzt, a.nzc)) {
     case 4: k_back_ref_dd<ZL, 4><<<dim3(tiles, 1, (nzt + 3) / 4), T::NT, 0, st>>>(a); break;
     case 2: k_back_ref_dd<ZL, 2><<<dim3(tiles, 1, (nzt + 1) / 2), T::NT, 0, st>>>(a); break;
     default: k_back_ref_dd<ZL, 1><<<dim3(tiles, 1, nzt), T::NT, 0, st>>>(a); break;
@@ -722,6 +729,7 @@ int make_back_dd_args(const Plan& p, int back_mode, const float* w, const ViewGe
     a.epi = epi;
     a.zt0 = zt0;
     a.nzt = nzt;
+    a.nzc = p.NZ;
     *ref = a;
     return nzt;
   }
@@ -734,6 +742,7 @@ int make_back_dd_args(const Plan& p, int back_mode, const float* w, const ViewGe
   a.ocx = p.ocx; a.ocy = p.ocy; a.dx = p.dx;
   a.zt0 = zt0;
   a.nzt = nzt;
+  a.nzc = p.NZ;
   // pass 1: x-major views along x columns -> tmp (mask applied)
   *pass1 = a;
   pass1->epi = epi;
@@ -1050,6 +1059,17 @@ DDFAN_API int ddfan_tune_set_zl(int zblocks, int zl) {
 }
 
 DDFAN_API int ddfan_tune_get_zl(int zblocks) { return zblocks < 1 ? 0 : pow2_zl(zblocks); }
+
+DDFAN_API int ddfan_tune_set_nz(int zblocks, int nz) {
+  if (zblocks < 1 || !(nz == 0 || nz == 1 || nz == 2 || nz == 4))
+    return set_err(DDFAN_ERR_ARG, "tune_set_nz: zblocks=%d nz=%d", zblocks, nz);
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  if (nz == 0) g_tuned_nz.erase(zblocks);
+  else g_tuned_nz[zblocks] = nz;
+  return DDFAN_OK;
+}
+
+DDFAN_API int ddfan_tune_get_nz(int zblocks) { return zblocks < 1 ? 0 : plan_nz(zblocks); }
 
 DDFAN_API size_t ddfan_plan_estimate_bytes(int XN, int YN, int DNU, int SLN, int PNmax, int sat_mode) {
   if (XN < 1 || YN < 1 || DNU < 2 || SLN < 1 || PNmax < 1 || sat_mode < 0 || sat_mode > SAT_DIRECT) return 0;

@@ -242,7 +242,7 @@ static int batch_create(Batch** out, Solver* const* solvers, int n) {
       r.ystride = s.Zi;
       const DdFwdArgs fa = make_fwd_dd_args(p, s.d_x, vg, fc, cvd, s.d_order + o, c, s.d_ax, s.U + 1, s.Zi, 0, s.Zi, &r);
       if (fa.nzt < 1) continue;
-      const int fnz = dd_nz(fa.nzt);
+      const int fnz = dd_nz(fa.nzt, fa.nzc);
       const int fi = (int)fargs.size();
       fargs.push_back(fa);
       const int cw = fwd_cw(p.ZL, fnz), ncb = (s.U + cw - 1) / cw, nzg = (fa.nzt + fnz - 1) / fnz;
@@ -269,7 +269,7 @@ static int batch_create(Batch** out, Solver* const* solvers, int n) {
       const int nzt = make_back_dd_args(p, s.back_mode, s.d_ax, vg, fc, s.d_order + o, s.d_counts + 2 * k, c, e, &a1,
                                         &a2, &ar);
       if (adj) {
-        const int bnz = dd_nz(nzt), nbz = (nzt + bnz - 1) / bnz;
+        const int bnz = dd_nz(nzt, p.NZ), nbz = (nzt + bnz - 1) / bnz;
         int LT, KT;
         adj_tile(p.ZL, &LT, &KT);
         const int i1 = (int)aargs.size();
@@ -284,7 +284,7 @@ static int batch_create(Batch** out, Solver* const* solvers, int n) {
         for (int zg = 0; zg < nbz; ++zg)
           for (int t = 0; t < ty; ++t) ly.push_back(make_int4(i1 + 1, t, zg, 0));
       } else {
-        const int bnz = dd_nz(nzt), nbz = (nzt + bnz - 1) / bnz;
+        const int bnz = dd_nz(nzt, p.NZ), nbz = (nzt + bnz - 1) / bnz;
         int LT, KT;
         adj_tile(p.ZL, &LT, &KT);  // the REF kernel uses the exact adjoint's voxel tile
         const int ri = (int)rargs.size();

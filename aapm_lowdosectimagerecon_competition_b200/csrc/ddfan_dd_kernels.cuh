@@ -101,6 +101,9 @@ __device__ __forceinline__ void ldg4_keep(bool p, const float4* a, float4& v) {
 // else it is cur), the first interior value only when there is one (n >= 2,
 // into vm, which otherwise keeps an earlier value under weight 0): about two
 // loads per footprint, and no branch unless it spans more than two steps.
+#ifndef DDFAN_WALK_LOADS_FIRST
+#define DDFAN_WALK_LOADS_FIRST 0
+#endif
 template <int NZ>
 __device__ __forceinline__ void walk_nz(float (&acc)[NZ][4], float4 (&cur)[NZ], float4 (&vm)[NZ],
                                         const float4* base, size_t stride, const int (&zoff)[NZ], int k0, int k1,
@@ -109,6 +112,22 @@ __device__ __forceinline__ void walk_nz(float (&acc)[NZ][4], float4 (&cur)[NZ], 
   const int km = min(max(k0 + st, 0), kmax);
   const float4* pm = base + (size_t)km * stride;
   const float4* pe = base + (size_t)k1 * stride;
+#if DDFAN_WALK_LOADS_FIRST
+  float4 ce[NZ];
+#pragma unroll
+  for (int z = 0; z < NZ; ++z) ce[z] = cur[z];
+#pragma unroll
+  for (int z = 0; z < NZ; ++z) ldg4_keep(n >= 2, pm + zoff[z], vm[z]);
+#pragma unroll
+  for (int z = 0; z < NZ; ++z) ldg4_keep(n >= 1, pe + zoff[z], ce[z]);
+#pragma unroll
+  for (int z = 0; z < NZ; ++z) {
+    fma4(acc[z], wt.x, cur[z]);
+    fma4(acc[z], wt.y, vm[z]);
+    fma4(acc[z], wt.z, ce[z]);
+    cur[z] = ce[z];
+  }
+#else
 #pragma unroll
   for (int z = 0; z < NZ; ++z) ldg4_keep(n >= 2, pm + zoff[z], vm[z]);
 #pragma unroll
@@ -120,6 +139,7 @@ __device__ __forceinline__ void walk_nz(float (&acc)[NZ][4], float4 (&cur)[NZ], 
     fma4(acc[z], wt.y, vm[z]);
     fma4(acc[z], wt.z, cur[z]);
   }
+#endif
   for (int i = 2; i < n; ++i) {
     const float4* pi = base + (size_t)(k0 + i * st) * stride;
 #pragma unroll
@@ -141,6 +161,7 @@ struct DdFwdArgs {
   int PN, U, Z, XN, YN;
   float dx;
   int zlo, zhi, zt0, nzt, row0;
+  int nzc;             // most z-tiles per thread (launch shape; the kernel reads NZ)
   // fused OS-SART residual (AAPM_script/OSSART_AAPM.m:86-88); y null = plain projection
   const float* y;      // measured [views][U][ystride]
   const int* yview;    // slot -> measured view
@@ -157,6 +178,11 @@ struct DdFwdArgs {
 #ifndef DDFAN_DD_FWD_GEOM
 #define DDFAN_DD_FWD_GEOM 256
 #endif
+// sums per chunk of lines added to the totals (1) or one running sum per
+// ray (0)
+#ifndef DDFAN_DD_FWD_PART
+#define DDFAN_DD_FWD_PART 1
+#endif
 // most z-tiles per thread (1, 2 or 4; fewer when a call has fewer)
 #ifndef DDFAN_DD_NZ
 #define DDFAN_DD_NZ 4
@@ -172,7 +198,8 @@ template <int ZL> struct DdFwdCG { static constexpr int v = ZL >= 4 ? DDFAN_DD_F
 // 4 slices per z-tile, so more z-tiles per thread means fewer instructions
 // per slice (the measured lever: 1 -> 4 took a 96-view c3 subset's forward
 // from 3.5 to 2.6 ms); at most the call's z-tiles
-inline int dd_nz(int nzt) { return nzt >= 4 && DDFAN_DD_NZ >= 4 ? 4 : (nzt >= 2 && DDFAN_DD_NZ >= 2 ? 2 : 1); }
+// (at most cap, the plan's tuned value)
+inline int dd_nz(int nzt, int cap) { return nzt >= 4 && cap >= 4 ? 4 : (nzt >= 2 && cap >= 2 ? 2 : 1); }
 
 template <int ZL, int CG, int NZ>
 struct DdFwdTile {
@@ -250,11 +277,15 @@ __device__ __forceinline__ void fwd_dd_body(const DdFwdArgs& a, int row, int cbl
     __syncwarp();
     if (active) {
       const int ncol = min(CC, nl - ii0);
+#if DDFAN_DD_FWD_PART
       float part[CG][NZ][4];
 #pragma unroll
       for (int j = 0; j < CG; ++j)
 #pragma unroll
         for (int z = 0; z < NZ; ++z) part[j][z][0] = part[j][z][1] = part[j][z][2] = part[j][z][3] = 0.f;
+#else
+      float (&part)[CG][NZ][4] = acc;
+#endif
 #pragma unroll(T::UNROLL)
       for (int col = 0; col < ncol; ++col) {
         const float4* line = img + (size_t)(ii0 + col) * lstride;
@@ -271,12 +302,14 @@ __device__ __forceinline__ void fwd_dd_body(const DdFwdArgs& a, int row, int cbl
           walk_nz<NZ>(part[j], cur, vm, line, kstride, zoff, pk & 0xffff, pk >> 16, N - 1, wt);
         }
       }
+#if DDFAN_DD_FWD_PART
 #pragma unroll
       for (int j = 0; j < CG; ++j)
 #pragma unroll
         for (int z = 0; z < NZ; ++z)
 #pragma unroll
           for (int s = 0; s < 4; ++s) acc[j][z][s] += part[j][z][s];
+#endif
     }
     __syncwarp();
   }
@@ -316,11 +349,12 @@ __device__ __forceinline__ void fwd_dd_body(const DdFwdArgs& a, int row, int cbl
 
 // Grid order of the forward: with DDFAN_DD_FWD_ROWS_X the view rows run
 // along grid x (dispatched first), so the CTAs in flight are every view of a
-// few channel blocks -- rays at one distance from the centre, whose image
-// footprint is an annulus -- instead of every channel block of a few views,
-// which spans the whole image.
+// few channel blocks -- rays at one distance from the centre, which miss the
+// disk inside it -- instead of every channel block of a few views.  On a c3
+// subset this cut the DRAM reads of the image from 2.05 to 1.33 GB per launch
+// (L2 hits 74 -> 82 %) and the launch from 2.36 to 2.15 ms.
 #ifndef DDFAN_DD_FWD_ROWS_X
-#define DDFAN_DD_FWD_ROWS_X 0
+#define DDFAN_DD_FWD_ROWS_X 1
 #endif
 
 // One CTA per (view row, channel block, z-tile group) of one call.
@@ -360,6 +394,7 @@ struct DdAdjArgs {
   double ocx, ocy, dx;
   BackEpi epi;
   int zt0, nzt;
+  int nzc;  // most z-tiles per thread (launch shape; the kernel reads NZ)
 };
 
 // pixels per thread of the direct exact adjoint
@@ -545,6 +580,7 @@ struct DdRefArgs {
   double ocx, ocy, dx, inv_sid, inv_dbeta, cnt;  // cnt = detCntIdx + 1 - 0.5
   BackEpi epi;
   int zt0, nzt;
+  int nzc;  // most z-tiles per thread (launch shape; the kernel reads NZ)
 };
 
 // The reference backprojector's formula (AAPM_script/MultiSlicesBackGPU.cu:

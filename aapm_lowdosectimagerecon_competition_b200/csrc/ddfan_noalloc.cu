@@ -133,6 +133,7 @@ extern "C" DDFAN_API int ddfan_proj_noalloc(float x0, float y0, int DNU, const f
   p.device = dev;
   p.XN = XN; p.YN = YN; p.U = DNU; p.Z = SLN; p.ZB = (SLN + 3) / 4;
   p.PNmax = PN; p.mode = sat_mode; p.ZL = plan_zl(p.ZB, 0);  // the z-tile width a plan would take
+  p.NZ = plan_nz(p.ZB);
   p.P4 = p.ZB;
   p.ZB = (p.ZB + p.ZL - 1) / p.ZL * p.ZL;
   p.x0 = x0; p.y0 = y0; p.dx = dx;

@@ -36,6 +36,7 @@ struct Plan {
   int device = 0;
   int XN = 0, YN = 0, U = 0, Z = 0, ZB = 0, PNmax = 0, mode = 0, ZL = 1;
   int P4 = 0;  // 4-slice blocks of the direct mode's operands: ceil(Z / 4)
+  int NZ = 4;  // most z-tiles per thread of the direct kernels (1, 2 or 4)
   double x0 = 0, y0 = 0, dx = 1, ocx = 0, ocy = 0, detCntIdx = 0;
   double inv_dbeta = 0, inv_sid = 0;  // REF backprojector
   double sh0x = 0, sh0y = -1;         // unit vector source -> rotation centre, angle 0
@@ -84,6 +85,9 @@ int pow2_zl(int ZB);
 // the z-tile width a plan uses: pow2_zl, narrowed by the DDFAN_ZL environment
 // variable (1, 2, 4 or 8), or exactly zl_force when that is one of those
 int plan_zl(int ZB, int zl_force);
+// most z-tiles per thread of the direct kernels for a stack of ZB blocks
+// (1, 2 or 4): the autotuner's record (ddfan_tune_set_nz), else 4
+int plan_nz(int ZB);
 // DD3Boundaries (AAPM_script/utilities.cuh:268-287), float-rounded like the reference stores them
 void boundaries(int n, const float* c, std::vector<double>& out);
 void plan_free(Plan* p);

@@ -1,8 +1,9 @@
 """Batched and served OS-SART reconstructions on one GPU.
 
 * `TileTuner` -- the autotuner: times the projector kernels for each
-  candidate z-tile width on a bucket's shape and records the fastest in the
-  library (ddfan_tune_set_zl) and in a JSON cache.
+  candidate tile shape (z-tile width; in the direct mode also the z-tiles a
+  thread walks) on a bucket's shape and records the fastest in the library
+  (ddfan_tune_set_zl, ddfan_tune_set_nz) and in a JSON cache.
 * `Engine` -- continuous batching: requests of uneven sizes are admitted, in
   arrival order with back-fill, while the HBM budget (exact per-request
   estimates from ddfan_ossart_estimate_bytes) and the slot count allow; every
@@ -103,31 +104,50 @@ def make_instance(N, Z, P, seed, device, iters=5, numOfOS=24, I0=1.5e5):
 # ---------------------------------------------------------------- autotuner
 
 class TileTuner:
-    """Measures every valid z-tile width for a slice count (4-slice blocks)
-    on a representative shape and keeps the fastest."""
+    """Measures every valid tile shape for a slice count (4-slice blocks) on
+    a representative shape and keeps the fastest: the z-tile width (z-lanes
+    per channel or voxel group, 1-8 blocks) and, in the direct mode, how many
+    z-tiles each thread walks per decoded footprint (1, 2 or 4)."""
 
-    def __init__(self, cache_path=None, sat="hilo"):
+    def __init__(self, cache_path=None, sat="hilo", back="adj"):
         self.cache_path = cache_path
         self.sat = sat
-        self.table = {}
+        self.back = back
+        self.table = {}    # zblocks -> [zl, nz] (nz 0: not tuned)
+        self.timings = {}  # zblocks -> {"zl,nz": ms}
         if cache_path and os.path.exists(cache_path):
             with open(cache_path) as f:
-                self.table = {int(k): int(v) for k, v in json.load(f).items()}
+                for k, v in json.load(f).items():
+                    self.table[int(k)] = [int(v), 0] if isinstance(v, int) else [int(v[0]), int(v[1])]
         self.apply()
 
     def apply(self):
         lib = load()
-        for zb, zl in self.table.items():
+        for zb, (zl, nz) in self.table.items():
             lib.ddfan_tune_set_zl(zb, zl)
+            lib.ddfan_tune_set_nz(zb, nz)
 
     def save(self):
         if self.cache_path:
             with open(self.cache_path, "w") as f:
                 json.dump({str(k): v for k, v in sorted(self.table.items())}, f, indent=1)
 
+    def candidates(self, zb):
+        """(zl, nz) pairs worth timing for zb blocks: every width that fits,
+        and in the direct mode every z-tiles-per-thread count its tiles allow."""
+        out = []
+        for zl in (8, 4, 2, 1):
+            if zl > zb:
+                continue
+            nzt = -(-zb // zl)
+            nzs = [nz for nz in (4, 2, 1) if nz == 1 or nzt >= nz] if self.sat == "direct" else [0]
+            out += [(zl, nz) for nz in nzs]
+        return out
+
     def tune(self, N, Z, P, device, reps=2):
-        """Returns the chosen width for Z slices; times forward + exact-adjoint
-        backprojection of P views on an N x N x Z image per candidate."""
+        """Returns the chosen [zl, nz] for Z slices (nz 0 outside the direct
+        mode); times forward + backprojection of P views on an N x N x Z image
+        per candidate."""
         lib = load()
         zb = (Z + 3) // 4
         if zb in self.table:
@@ -138,30 +158,31 @@ class TileTuner:
         angs = torch.from_numpy(s.angles(P)).to(device)
         vol = torch.rand((N, N, Z), device=device) * 0.02
         best, best_ms, timings = None, float("inf"), {}
-        for zl in (8, 4, 2, 1):
-            if zl > zb:
-                continue
+        for zl, nz in self.candidates(zb):
             lib.ddfan_tune_set_zl(zb, zl)
+            lib.ddfan_tune_set_nz(zb, nz)
             pl = Plan(x0, y0, s.DNU, xds, yds, s.detCntIdx, N, N, Z, P, dx, sat=self.sat,
                       device=device.index)
             prj = pl.proj(angs, vol)
             out = torch.empty_like(vol)
-            pl.back(angs, prj, out=out, mode="adj")
+            pl.back(angs, prj, out=out, mode=self.back)
             torch.cuda.synchronize(device)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             for _ in range(reps):
                 pl.proj(angs, vol, out=prj)
-                pl.back(angs, prj, out=out, mode="adj")
+                pl.back(angs, prj, out=out, mode=self.back)
             e1.record()
             torch.cuda.synchronize(device)
             ms = e0.elapsed_time(e1) / reps
-            timings[zl] = ms
+            timings["%d,%d" % (zl, nz)] = round(ms, 4)
             pl.close()
             if ms < best_ms:
-                best, best_ms = zl, ms
-        lib.ddfan_tune_set_zl(zb, best)
+                best, best_ms = [zl, nz], ms
+        lib.ddfan_tune_set_zl(zb, best[0])
+        lib.ddfan_tune_set_nz(zb, best[1])
         self.table[zb] = best
+        self.timings[zb] = timings
         return best
 
 

@@ -72,7 +72,7 @@ def parse():
 def _c4_instances(args, dev, iters):
     from aapm_lowdosectimagerecon_competition_b200 import configs, serve
     sizes = configs.c4_instances(args.instances)
-    tuner = serve.TileTuner(sat=args.sat)
+    tuner = serve.TileTuner(sat=args.sat, back=args.back)
     for zb in sorted({(Z + 3) // 4 for _, Z, _ in sizes}):
         tuner.tune(N=512, Z=4 * zb, P=96, device=dev, reps=1)
     insts = [serve.make_instance(N, Z, P, seed=100 + i, device=dev, iters=iters)
@@ -114,7 +114,8 @@ def run_c4(args):
             "batched": batched, "streams": res["streams"], "serial": res["serial"],
             "speedup_vs_serial": best["iters_per_s"] / res["serial"]["iters_per_s"],
             "streams_vs_serial": res["streams"]["iters_per_s"] / res["serial"]["iters_per_s"],
-            "tile_table": tuner.table, "sat": args.sat, "back": args.back, "data": "synthetic"}
+            "tile_table": {zb: {"zl": v[0], "nz": v[1]} for zb, v in sorted(tuner.table.items())},
+            "tile_timings_ms": tuner.timings, "sat": args.sat, "back": args.back, "data": "synthetic"}
     print(json.dumps(line), flush=True)
 
 

@@ -63,6 +63,12 @@ DDFAN_API int ddfan_version(void);
  * created afterwards. */
 DDFAN_API int ddfan_tune_set_zl(int zblocks, int zl);
 DDFAN_API int ddfan_tune_get_zl(int zblocks);
+/* the direct mode's (DDFAN_SAT_DIRECT) second tile dimension: each thread
+ * walks the footprints it decodes for up to nz z-tiles (nz in {1, 2, 4};
+ * default 4; nz = 0 forgets a record).  Results do not depend on it (every
+ * slice sums the same terms in the same order); the launch shape does. */
+DDFAN_API int ddfan_tune_set_nz(int zblocks, int nz);
+DDFAN_API int ddfan_tune_get_nz(int zblocks);
 /* device bytes ddfan_plan_create / ddfan_ossart_create would allocate
  * (the solver figure includes its transient set-up buffers); 0 = bad sizes.
  * Both are for one angle list shared by all slices.  Per-slice lists take

@@ -470,3 +470,34 @@ def test_slice_major_kernels_at_768_pixel_lines(mods, back):
     eb = O.back(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0, 0, h, PN, s.XN, s.YN, s.SLN, prj, s.dx,
                 mode=O.ADJ if back == "adj" else O.REF)
     assert rel(gb, eb) < 2e-6
+
+
+def test_direct_results_do_not_depend_on_z_tiles_per_thread(mods):
+    """The autotuner's second dimension in the direct mode (z-tiles a thread
+    walks per decoded footprint, ddfan_tune_set_nz) changes the launch shape
+    only: every slice sums the same terms in the same order, so projections
+    and both backprojections are bit-identical for 4, 2 and 1."""
+    import torch
+    from aapm_lowdosectimagerecon_competition_b200._lib import load
+    dd2, configs, device, O = mods
+    lib = load()
+    g, vol, prj = make_case(configs, dd2, SLN=150, XN=36, YN=30, PN=40, masked=True)
+    zb = (g["SLN"] + 3) // 4
+    angs = torch.from_numpy(np.ascontiguousarray(g["h"][:, 0])).cuda()
+    vt, pt = torch.from_numpy(vol).cuda(), torch.from_numpy(prj).cuda()
+    outs = {}
+    try:
+        for nz in (4, 2, 1):
+            assert lib.ddfan_tune_set_nz(zb, nz) == 0
+            assert lib.ddfan_tune_get_nz(zb) == nz
+            pl = device.Plan(g["x0"], g["y0"], g["DNU"], g["xds"], g["yds"], g["cnt"], g["XN"], g["YN"],
+                             g["SLN"], g["PN"], g["dx"], mask=g["mask"], sat="direct")
+            outs[nz] = [pl.proj(angs, vt).cpu().numpy(), pl.back(angs, pt, mode="adj").cpu().numpy(),
+                        pl.back(angs, pt, mode="ref").cpu().numpy()]
+            pl.close()
+    finally:
+        lib.ddfan_tune_set_nz(zb, 0)
+    for nz in (2, 1):
+        for a, b in zip(outs[4], outs[nz]):
+            np.testing.assert_array_equal(a, b)
+    assert rel(outs[4][0], ofwd(O, g, vol)) < TOL["direct"]

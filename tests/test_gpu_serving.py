@@ -70,6 +70,27 @@ def test_tuner_records_a_valid_width(setup):
     from aapm_lowdosectimagerecon_competition_b200._lib import load
     lib = load()
     t = serve.TileTuner()
-    zl = t.tune(N=64, Z=32, P=48, device=dev, reps=1)
-    assert zl in (1, 2, 4, 8) and lib.ddfan_tune_get_zl(8) == zl
+    zl, nz = t.tune(N=64, Z=32, P=48, device=dev, reps=1)
+    assert zl in (1, 2, 4, 8) and nz == 0 and lib.ddfan_tune_get_zl(8) == zl
     lib.ddfan_tune_set_zl(8, 0)
+
+
+def test_tuner_records_a_shape_in_the_direct_mode(setup, tmp_path):
+    torch, serve, dev, insts = setup
+    from aapm_lowdosectimagerecon_competition_b200._lib import load
+    lib = load()
+    cache = str(tmp_path / "tiles.json")
+    t = serve.TileTuner(cache_path=cache, sat="direct", back="ref")
+    zl, nz = t.tune(N=64, Z=64, P=48, device=dev, reps=1)
+    # 16 blocks: widths 8, 4, 2, 1 with every z-tiles-per-thread count that fits
+    assert len(t.timings[16]) == 2 + 3 + 3 + 3
+    assert zl in (1, 2, 4, 8) and nz in (1, 2, 4)
+    assert lib.ddfan_tune_get_zl(16) == zl and lib.ddfan_tune_get_nz(16) == nz
+    t.save()
+    lib.ddfan_tune_set_zl(16, 0)
+    lib.ddfan_tune_set_nz(16, 0)
+    assert lib.ddfan_tune_get_nz(16) == 4
+    serve.TileTuner(cache_path=cache, sat="direct")  # re-applies the cached record
+    assert lib.ddfan_tune_get_zl(16) == zl and lib.ddfan_tune_get_nz(16) == nz
+    lib.ddfan_tune_set_zl(16, 0)
+    lib.ddfan_tune_set_nz(16, 0)

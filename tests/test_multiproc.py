@@ -61,6 +61,28 @@ def test_slabs_match_reference_start_indices():
         assert shard.slice_slab(SLN, n - 1, n)[1] == SLN
 
 
+def test_tuner_candidates_and_cache(tmp_path):
+    # host logic only: the candidate tile shapes and the cache format
+    direct = serve.TileTuner(sat="direct")
+    assert direct.candidates(16) == [(8, 2), (8, 1), (4, 4), (4, 2), (4, 1), (2, 4), (2, 2), (2, 1),
+                                     (1, 4), (1, 2), (1, 1)]
+    assert direct.candidates(2) == [(2, 1), (1, 2), (1, 1)]
+    assert serve.TileTuner(sat="hilo").candidates(4) == [(4, 0), (2, 0), (1, 0)]
+    cache = tmp_path / "tiles.json"
+    cache.write_text('{"3": 2, "16": [4, 2]}')  # a width-only record and a width + z-tiles record
+    t = serve.TileTuner(cache_path=str(cache), sat="direct")
+    assert t.table == {3: [2, 0], 16: [4, 2]}
+    lib = serve.load()
+    try:
+        assert lib.ddfan_tune_get_zl(3) == 2 and lib.ddfan_tune_get_zl(16) == 4
+        assert lib.ddfan_tune_get_nz(16) == 2 and lib.ddfan_tune_get_nz(3) == 4
+        assert lib.ddfan_tune_set_nz(16, 3) != 0
+    finally:
+        for zb in (3, 16):
+            lib.ddfan_tune_set_zl(zb, 0)
+            lib.ddfan_tune_set_nz(zb, 0)
+
+
 def test_admission_policy():
     gb = 1e9
     # oldest that fits within the look-ahead window
