@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-modes", action="store_true",
+                    help="skip the other precision / backprojector modes timed beside the headline")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the final-image check against the FP64 oracle (and the CPU baseline it times)")
     ap.add_argument("--kernels", action="store_true",
@@ -827,6 +829,16 @@ def run_ours(args):
     if not args.no_plain and rank == 0:
         line["plain_fp32"] = plain_fp32_iteration(s, (x0, y0, xds, yds), y, mask)
 
+    # ---- the same iteration in the other modes (compensated tables, the exact adjoint)
+    if not args.no_modes and rank == 0 and args.views == "shared":
+        modes = {}
+        for sat, back in (("hilo", "ref"), ("hilo", "adj"), ("direct", "adj"), ("direct", "ref")):
+            if (sat, back) != (args.sat, args.back):
+                modes["%s/%s" % (sat, back)] = mode_rate(s, (x0, y0, xds, yds), y, mask, hangs, sat, back, local)
+        line["other_modes"] = {"iters_per_s": modes,
+                               "how": "the same workload and sinogram, 2 warm-up and 5 timed graph replays "
+                                      "per mode (sat/back); hilo = compensated prefix-sum tables"}
+
     # ---- final-image parity at this configuration, and the CPU baseline
     parity_failed = False
     if rank == 0 and not args.no_parity:
@@ -896,6 +908,28 @@ def _ossart_host(s, geom, y_h, x_h, out_h, mask, iters, args):
     call("ddfan_OSSART_AAPM", x0, y0, s.DNU, P(xds), P(yds), s.detCntIdx, 0.0, 0.0, T(y_h), P(hangs),
          s.PN, s.XN, s.YN, s.SLN, s.dx, T(x_h), P(m), iters, s.numOfOS, s.useFISTA, s.nonneg,
          SAT_MODES[args.sat], BACK_MODES[args.back], T(out_h))
+
+
+def mode_rate(s, geom, y, mask, hangs, sat, back, local, steps=5):
+    """OS-SART iterations/s of one solver mode on the bench workload."""
+    import torch
+    from aapm_lowdosectimagerecon_competition_b200 import device
+    x0, y0, xds, yds = geom
+    sv = device.OSSART(x0, y0, s.DNU, xds, yds, s.detCntIdx, hangs, s.XN, s.YN, s.SLN, s.dx,
+                       mask=mask, numOfOS=s.numOfOS, useFISTA=s.useFISTA, nonneg=s.nonneg,
+                       sat=sat, back=back, device=local)
+    sv.set_sinogram(y)
+    sv.set_image(torch.zeros((s.YN, s.XN, s.SLN), device=y.device))
+    st = torch.cuda.current_stream(y.device)
+    sv.iterate(2, use_graph=True, stream=st)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(y.device)
+    e0.record(st)
+    sv.iterate(steps, use_graph=True, stream=st)
+    e1.record(st)
+    torch.cuda.synchronize(y.device)
+    sv.close()
+    return round(steps / (e0.elapsed_time(e1) / 1e3), 3)
 
 
 def plain_fp32_iteration(s, geom, y, mask):
