@@ -884,11 +884,25 @@ def parity_check(s, geom, y, mask, hangs, solver, stream, args):
     xo, secs = O.ossart(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0.0, 0.0, hs, s.PN, s.XN, s.YN, len(pick), ys, init,
                         s.dx, mask, iters, s.numOfOS, s.useFISTA, s.nonneg,
                         back_mode=O.ADJ if args.back == "adj" else O.REF, nthreads=nt, timing=True)
-    d = xg[:, :, pick] - xo
-    rel = float(np.linalg.norm(d.ravel()) / np.linalg.norm(xo.ravel()))
-    par = {"rel_l2": rel, "max_abs": float(np.abs(d).max()), "image_max": float(np.abs(xo).max()),
-           "slices": pick, "iterations": iters, "bound": PARITY_BOUND, "ok": rel <= PARITY_BOUND,
+    # With per-slice angle lists the reference's update diverges on every slice
+    # whose rays differ from slice 0's: the row sums are slice 0's
+    # (OSSART_AAPM.m:63), and where a row sum is 0 the residual is replaced by
+    # A x itself (:88), so rays that miss slice 0's masked disk but cross this
+    # slice's feed the image back into itself.  The bound then applies to
+    # slice 0; the other slice is reported (both solves blow up alike).
+    bounded = pick if args.views == "shared" else pick[:1]
+    sel = [pick.index(z) for z in bounded]
+    d = xg[:, :, bounded] - xo[:, :, sel]
+    rel = float(np.linalg.norm(d.ravel()) / np.linalg.norm(xo[:, :, sel].ravel()))
+    par = {"rel_l2": rel, "max_abs": float(np.abs(d).max()), "image_max": float(np.abs(xo[:, :, sel]).max()),
+           "slices": bounded, "iterations": iters, "bound": PARITY_BOUND, "ok": rel <= PARITY_BOUND,
            "against": "FP64 CPU oracle (oracle/ddfan_oracle.c), same sinogram, from zero"}
+    if bounded != pick:
+        z = pick[-1]
+        par["diverging_slice"] = {
+            "slice": z, "oracle_max": float(np.abs(xo[:, :, -1]).max()), "gpu_max": float(np.abs(xg[:, :, z]).max()),
+            "why": "slice-0 row sums for every slice and A x kept where a row sum is 0 "
+                   "(AAPM_script/OSSART_AAPM.m:63, :88) feed back on this slice's rays"}
     per_iter = secs / iters
     cpu = {"value": 1.0 / (per_iter * s.SLN / len(pick)), "unit": UNIT, "cores": nt, "kind": "port",
            "sample": "%d OS-SART iterations (%d subsets, %d views, FP64, %s) on slices %s of %d, per-iteration "

@@ -211,3 +211,27 @@ def test_fan_geometry_restatement_matches_matlab_formula():
     np.testing.assert_allclose(xds, 1085.6 * np.sin(beta), rtol=0, atol=2e-4)
     np.testing.assert_allclose(yds, 595.0 - 1085.6 * np.cos(beta), rtol=0, atol=2e-4)
     assert x0 == 0 and y0 == np.float32(595.0)
+
+
+def test_reference_update_diverges_with_per_slice_lists():
+    """A finding about the reference's OS-SART, not about the kernels: it takes
+    slice 0's row and column sums for every slice (OSSART_AAPM.m:63-64) and
+    keeps A x where a row sum is 0 (:88).  With one angle list per slice (as
+    rebinning makes them) a rotated slice has rays that cross the masked disk
+    where slice 0's rays miss it, and those rays feed the image back into
+    itself: one iteration takes slice 77 to ~80x the phantom's maximum while
+    slice 0 stays bounded, for both backprojectors.  The solvers reproduce
+    this, so per-slice parity is bounded on slice 0."""
+    from aapm_lowdosectimagerecon_competition_b200 import configs
+    s = configs.scaled(configs.c3(SLN=128), XN=64, PN=576, DNU=184)
+    s.numOfOS = 8
+    x0, y0, xds, yds = N.fan_geometry(s.sid, s.sdd, s.DNU, s.detCellWidth, s.detCntIdx)
+    hs = np.ascontiguousarray(s.rebinned_hangs(spacing=86.07 * 576 / 2304)[:, [0, 77]])
+    xt = np.ascontiguousarray(configs.phantom(s)[:, :, [0, 77]])
+    y = O.proj(x0, y0, s.DNU, xds, yds, 0, 0, hs, s.PN, s.XN, s.YN, 2, xt, s.dx, None).astype(np.float32)
+    for back in (O.REF, O.ADJ):
+        x = O.ossart(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0.0, 0.0, hs, s.PN, s.XN, s.YN, 2, y,
+                     np.zeros_like(xt), s.dx, s.circular_mask(), 1, s.numOfOS, 1, 1, back_mode=back, nthreads=4)
+        top = np.abs(x).reshape(-1, 2).max(0)
+        assert top[0] < 1.5 * xt.max()
+        assert top[1] > 20 * xt.max()
