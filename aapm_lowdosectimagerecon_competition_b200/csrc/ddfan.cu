@@ -228,6 +228,25 @@ void boundaries(int n, const float* c, std::vector<double>& out) {
   }
 }
 
+// The direct forward kernels' dynamic shared memory, allowed on the current
+// device (dev, for the message) at every plan creation -- a kernel
+// attribute belongs to the context, which a device reset replaces.  Plan
+// creation precedes every launch on a plan and never runs under capture.
+int dd_prepare_device(int dev) {
+  cudaError_t e = cudaSuccess;
+#define DDFAN_DD_ALLOW(ZLv, NZv)                                                                  \
+  if (e == cudaSuccess)                                                                           \
+    e = dd_allow_dyn(k_fwd_dd<ZLv, DdFwdCG<ZLv>::v, NZv>, DdFwdTile<ZLv, DdFwdCG<ZLv>::v, NZv>::DYN);
+  DDFAN_DD_ALLOW(8, 4) DDFAN_DD_ALLOW(8, 2) DDFAN_DD_ALLOW(8, 1)
+  DDFAN_DD_ALLOW(4, 4) DDFAN_DD_ALLOW(4, 2) DDFAN_DD_ALLOW(4, 1)
+  DDFAN_DD_ALLOW(2, 4) DDFAN_DD_ALLOW(2, 2) DDFAN_DD_ALLOW(2, 1)
+  DDFAN_DD_ALLOW(1, 4) DDFAN_DD_ALLOW(1, 2) DDFAN_DD_ALLOW(1, 1)
+#undef DDFAN_DD_ALLOW
+  if (e != cudaSuccess)
+    return set_err(DDFAN_ERR_CUDA, "forward kernel attributes on device %d: %s", dev, cudaGetErrorString(e));
+  return DDFAN_OK;
+}
+
 int plan_create(Plan** out, const PlanDesc& d) {
   *out = nullptr;
   if (d.DNU < 2 || d.XN < 1 || d.YN < 1 || d.SLN < 1 || d.PNmax < 1 || !d.xds || !d.yds)
@@ -246,6 +265,13 @@ int plan_create(Plan** out, const PlanDesc& d) {
   int prev = -1;
   cudaGetDevice(&prev);
   if (cudaSetDevice(d.device) != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "cudaSetDevice(%d)", d.device);
+  {
+    const int rc = dd_prepare_device(d.device);
+    if (rc) {
+      if (prev >= 0) cudaSetDevice(prev);
+      return rc;
+    }
+  }
   std::unique_ptr<Plan, void (*)(Plan*)> P(new Plan(), plan_free);
   Plan& p = *P;
   p.device = d.device;
@@ -640,7 +666,7 @@ static void fwd_dd_go(const DdFwdArgs& a, int nzt, cudaStream_t st) {
       b.row0 = r0;
       const int rows = std::min(a.PN - r0, kMaxRows), cblk = (a.U + T::CW - 1) / T::CW;
       const dim3 grid(DDFAN_DD_FWD_ROWS_X ? rows : cblk, DDFAN_DD_FWD_ROWS_X ? cblk : rows, (nzt + NZ - 1) / NZ);
-      k_fwd_dd<ZL, CG, NZ><<<grid, T::NT, 0, st>>>(b);
+      k_fwd_dd<ZL, CG, NZ><<<grid, T::NT, T::DYN, st>>>(b);
     }
   };
   switch (dd_nz(nzt, a.nzc)) {

@@ -70,7 +70,7 @@ void adj_tile(int ZL, int* LT, int* KT) {
 
 template <int ZL, int NZ>
 void go_fwd(const DdFwdArgs* a, const int4* it, unsigned n, cudaStream_t st) {
-  k_fwd_dd_batch<ZL, DdFwdCG<ZL>::v, NZ><<<n, 256, 0, st>>>(a, it);
+  k_fwd_dd_batch<ZL, DdFwdCG<ZL>::v, NZ><<<n, 256, DdFwdTile<ZL, DdFwdCG<ZL>::v, NZ>::DYN, st>>>(a, it);
 }
 
 template <int ZL, int NZ>
@@ -82,6 +82,23 @@ void go_adj(bool xm, const DdAdjArgs* a, const int4* it, unsigned n, cudaStream_
 template <int ZL, int NZ>
 void go_ref(const DdRefArgs* a, const int4* it, unsigned n, cudaStream_t st) {
   k_back_ref_dd_batch<ZL, NZ><<<n, 256, 0, st>>>(a, it);
+}
+
+// the work-list forward kernels' dynamic shared memory on the current device
+// (at every batch creation: the attribute belongs to the context)
+int batch_prepare_device(int dev) {
+  cudaError_t e = cudaSuccess;
+#define DDFAN_DD_ALLOW(ZLv, NZv)                                                                        \
+  if (e == cudaSuccess)                                                                                 \
+    e = dd_allow_dyn(k_fwd_dd_batch<ZLv, DdFwdCG<ZLv>::v, NZv>, DdFwdTile<ZLv, DdFwdCG<ZLv>::v, NZv>::DYN);
+  DDFAN_DD_ALLOW(8, 4) DDFAN_DD_ALLOW(8, 2) DDFAN_DD_ALLOW(8, 1)
+  DDFAN_DD_ALLOW(4, 4) DDFAN_DD_ALLOW(4, 2) DDFAN_DD_ALLOW(4, 1)
+  DDFAN_DD_ALLOW(2, 4) DDFAN_DD_ALLOW(2, 2) DDFAN_DD_ALLOW(2, 1)
+  DDFAN_DD_ALLOW(1, 4) DDFAN_DD_ALLOW(1, 2) DDFAN_DD_ALLOW(1, 1)
+#undef DDFAN_DD_ALLOW
+  if (e != cudaSuccess)
+    return set_err(DDFAN_ERR_CUDA, "batched forward kernel attributes on device %d: %s", dev, cudaGetErrorString(e));
+  return DDFAN_OK;
 }
 
 #define DDFAN_BATCH_ZL_NZ(ZLv, NZv, CALL) \
@@ -218,6 +235,10 @@ static int batch_create(Batch** out, Solver* const* solvers, int n) {
   }
   b.device = solvers[0]->device;
   DeviceGuard g(b.device);
+  {
+    const int rc = batch_prepare_device(b.device);
+    if (rc) return rc;
+  }
   int maxsub = 0;
   for (Solver* s : b.sv) maxsub = std::max(maxsub, s->nsub);
   std::vector<DdFwdArgs> fargs;

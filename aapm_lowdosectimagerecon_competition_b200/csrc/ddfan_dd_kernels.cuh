@@ -178,19 +178,27 @@ struct DdFwdArgs {
 #ifndef DDFAN_DD_FWD_GEOM
 #define DDFAN_DD_FWD_GEOM 256
 #endif
-// sums per chunk of lines added to the totals (1) or one running sum per
-// ray (0)
+// Ray sums: 0 = one running FP32 sum per ray; 1 = a sum per chunk of
+// lines in registers, added to the totals, also in registers; 2 = chunk sums
+// in registers, totals in dynamic shared memory (one slot per thread and
+// value, so a chunk's sum is added with one load and one store per value).
+// Chunk sums keep a 512-line ray's rounding at the level of ~CC terms; in
+// registers they spill two channels per thread, in shared memory they cost
+// the registers nothing.
 #ifndef DDFAN_DD_FWD_PART
-#define DDFAN_DD_FWD_PART 1
+#define DDFAN_DD_FWD_PART 2
 #endif
 // most z-tiles per thread (1, 2 or 4; fewer when a call has fewer)
 #ifndef DDFAN_DD_NZ
 #define DDFAN_DD_NZ 4
 #endif
 
-// channels per thread of the direct forward projector for a z-lane count
+// channels per thread of the direct forward projector for a z-lane count:
+// two share the boundary value between them and the per-line decode
+// (c3 subset: 2.16 -> 1.90 ms with one running sum per ray; with chunk sums
+// the extra registers spill and the gain is gone)
 #ifndef DDFAN_DD_FWD_CG
-#define DDFAN_DD_FWD_CG 1
+#define DDFAN_DD_FWD_CG 2
 #endif
 template <int ZL> struct DdFwdCG { static constexpr int v = ZL >= 4 ? DDFAN_DD_FWD_CG : (ZL == 2 ? 2 : 1); };
 
@@ -209,6 +217,8 @@ struct DdFwdTile {
   static constexpr int CW = NW * CWW;                 // channels per CTA
   static constexpr int CC = DDFAN_DD_FWD_GEOM / CWW;  // lines per geometry chunk
   static constexpr int UNROLL = DDFAN_DD_FWD_UNROLL;
+  // dynamic shared memory of the ray totals (DDFAN_DD_FWD_PART == 2)
+  static constexpr int DYN = DDFAN_DD_FWD_PART == 2 ? CG * NZ * 4 * NT * (int)sizeof(float) : 0;
 };
 
 // CTA = one view x CW channels x NZ z-tiles of 4*ZL slices; a thread owns CG
@@ -260,6 +270,12 @@ __device__ __forceinline__ void fwd_dd_body(const DdFwdArgs& a, int row, int cbl
     for (int z = 0; z < NZ; ++z) acc[j][z][0] = acc[j][z][1] = acc[j][z][2] = acc[j][z][3] = 0.f;
   const double Nd = (double)N;
   const float dx = a.dx;
+#if DDFAN_DD_FWD_PART == 2
+  extern __shared__ float s_tot[];  // [CG * NZ * 4][NT]: this thread's totals at tid
+  float* tot = s_tot + tid;
+#pragma unroll
+  for (int e = 0; e < CG * NZ * 4; ++e) tot[e * T::NT] = 0.f;
+#endif
   __syncwarp();
   for (int ii0 = 0; ii0 < nl; ii0 += CC) {
     for (int e = lane; e < CC * CWW; e += 32) {
@@ -277,7 +293,7 @@ __device__ __forceinline__ void fwd_dd_body(const DdFwdArgs& a, int row, int cbl
     __syncwarp();
     if (active) {
       const int ncol = min(CC, nl - ii0);
-#if DDFAN_DD_FWD_PART
+#if DDFAN_DD_FWD_PART == 1
       float part[CG][NZ][4];
 #pragma unroll
       for (int j = 0; j < CG; ++j)
@@ -302,18 +318,37 @@ __device__ __forceinline__ void fwd_dd_body(const DdFwdArgs& a, int row, int cbl
           walk_nz<NZ>(part[j], cur, vm, line, kstride, zoff, pk & 0xffff, pk >> 16, N - 1, wt);
         }
       }
-#if DDFAN_DD_FWD_PART
+#if DDFAN_DD_FWD_PART == 1
 #pragma unroll
       for (int j = 0; j < CG; ++j)
 #pragma unroll
         for (int z = 0; z < NZ; ++z)
 #pragma unroll
           for (int s = 0; s < 4; ++s) acc[j][z][s] += part[j][z][s];
+#elif DDFAN_DD_FWD_PART == 2
+#pragma unroll
+      for (int j = 0; j < CG; ++j)
+#pragma unroll
+        for (int z = 0; z < NZ; ++z)
+#pragma unroll
+          for (int s = 0; s < 4; ++s) {
+            float* t = tot + ((j * NZ + z) * 4 + s) * T::NT;
+            *t += acc[j][z][s];
+            acc[j][z][s] = 0.f;
+          }
 #endif
     }
     __syncwarp();
   }
   if (!active) return;
+#if DDFAN_DD_FWD_PART == 2
+#pragma unroll
+  for (int j = 0; j < CG; ++j)
+#pragma unroll
+    for (int z = 0; z < NZ; ++z)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) acc[j][z][s] = tot[((j * NZ + z) * 4 + s) * T::NT];
+#endif
 #pragma unroll
   for (int j = 0; j < CG; ++j) {
     const int u = wc0 + gw * CG + j;
@@ -356,6 +391,14 @@ __device__ __forceinline__ void fwd_dd_body(const DdFwdArgs& a, int row, int cbl
 #ifndef DDFAN_DD_FWD_ROWS_X
 #define DDFAN_DD_FWD_ROWS_X 1
 #endif
+
+// Allows a forward kernel its dynamic shared memory on the current device
+// (above the 48 KB default with the static arrays).  Host-side, once per
+// device, before any launch or capture.
+template <typename K>
+inline cudaError_t dd_allow_dyn(K kernel, int bytes) {
+  return bytes > 0 ? cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) : cudaSuccess;
+}
 
 // One CTA per (view row, channel block, z-tile group) of one call.
 template <int ZL, int CG, int NZ>

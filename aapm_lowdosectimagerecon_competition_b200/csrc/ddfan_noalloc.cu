@@ -78,6 +78,9 @@ int scratch_address(int dev, unsigned char** out) {
       cudaGetLastError();
       return set_err(DDFAN_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
     }
+    // the direct forward kernels' shared memory limit, set in this context too
+    const int rc = dd_prepare_device(dev);
+    if (rc) return rc;
     g_addr[dev] = p;
     // the lookup made the device's context current if none was
     g_ctx_id[dev] = current_context_id();

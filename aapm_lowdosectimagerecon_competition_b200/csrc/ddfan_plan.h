@@ -88,6 +88,9 @@ int plan_zl(int ZB, int zl_force);
 // most z-tiles per thread of the direct kernels for a stack of ZB blocks
 // (1, 2 or 4): the autotuner's record (ddfan_tune_set_nz), else 4
 int plan_nz(int ZB);
+// allows the direct forward kernels their dynamic shared memory on the
+// current device (dev names it in an error); before any launch there
+int dd_prepare_device(int dev);
 // DD3Boundaries (AAPM_script/utilities.cuh:268-287), float-rounded like the reference stores them
 void boundaries(int n, const float* c, std::vector<double>& out);
 void plan_free(Plan* p);

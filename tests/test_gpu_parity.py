@@ -501,3 +501,28 @@ def test_direct_results_do_not_depend_on_z_tiles_per_thread(mods):
         for a, b in zip(outs[4], outs[nz]):
             np.testing.assert_array_equal(a, b)
     assert rel(outs[4][0], ofwd(O, g, vol)) < TOL["direct"]
+
+
+@pytest.mark.parametrize("N", [768, 1024])
+def test_direct_kernels_at_long_lines(mods, N):
+    """The direct mode sums each ray in one FP32 running sum over its lines
+    (no chunk sums): at the longest lines a plan takes (1024 pixels) the
+    projection and both backprojections stay within the 2e-6 bound of the
+    FP64 oracle."""
+    dd2, configs, device, O = mods
+    s = configs.c2(SLN=8)
+    s.dx = 0.7 * 512 / N
+    s.XN = s.YN = N
+    PN = 24
+    x0, y0, xds, yds = dd2.fan_geometry(s.sid, s.sdd, s.DNU, s.detCellWidth, s.detCntIdx)
+    h = np.repeat(s.angles(PN)[:, None], s.SLN, 1).astype(np.float32)
+    vol = configs.ellipsoid_phantom_3d(s)
+    prj = np.random.default_rng(8).random((PN, s.DNU, s.SLN)).astype(np.float32)
+    got = dd2.MultiSlicesProjGPU(x0, y0, s.DNU, xds, yds, 0, 0, h, PN, s.XN, s.YN, s.SLN, vol, s.dx, sat="direct")
+    exp = O.proj(x0, y0, s.DNU, xds, yds, 0, 0, h, PN, s.XN, s.YN, s.SLN, vol, s.dx)
+    assert rel(got, exp) < 2e-6
+    for back, mode in (("adj", O.ADJ), ("ref", O.REF)):
+        gb = dd2.MultiSlicesBackGPU(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0, 0, h, PN, s.XN, s.YN, s.SLN, prj,
+                                    s.dx, sat="direct", back=back)
+        eb = O.back(x0, y0, s.DNU, xds, yds, s.detCntIdx, 0, 0, h, PN, s.XN, s.YN, s.SLN, prj, s.dx, mode=mode)
+        assert rel(gb, eb) < 2e-6
