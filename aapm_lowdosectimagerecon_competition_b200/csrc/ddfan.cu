@@ -102,6 +102,10 @@ int pow2_zl(int ZB) {
 }
 
 int plan_nz(int ZB) {
+  if (const char* v = getenv("DDFAN_NZ")) {  // a fixed value for measurements, like DDFAN_ZL
+    const int nz = atoi(v);
+    if (nz == 1 || nz == 2 || nz == 4) return nz;
+  }
   std::lock_guard<std::mutex> lock(g_tune_mutex);
   auto it = g_tuned_nz.find(ZB);
   return it == g_tuned_nz.end() ? DDFAN_DD_NZ : it->second;

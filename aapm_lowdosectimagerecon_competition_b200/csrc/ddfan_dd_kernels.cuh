@@ -37,6 +37,18 @@ namespace ddfan {
 #ifndef DDFAN_DD_BACK_MIN_CTAS
 #define DDFAN_DD_BACK_MIN_CTAS 2
 #endif
+// With DDFAN_DD_MIN_CTAS_BY_NZ the kernels of fewer z-tiles per thread (fewer
+// accumulators) are built for one (NZ = 2: 80 registers) or two (NZ = 1: 64)
+// more resident CTAs.  On a c3 subset forced to NZ = 2 this took the forward
+// from 2.84 to 2.28 ms and the REF backprojector from 2.03 to 1.80 (NZ = 1:
+// 3.59 -> 3.00, 3.56 -> 2.82); the NZ = 4 kernels are unchanged.
+#ifndef DDFAN_DD_MIN_CTAS_BY_NZ
+#define DDFAN_DD_MIN_CTAS_BY_NZ 1
+#endif
+template <int NZ, int BASE>
+struct DdMinCtas {
+  static constexpr int v = DDFAN_DD_MIN_CTAS_BY_NZ ? (NZ >= 4 ? BASE : (NZ == 2 ? BASE + 1 : BASE + 2)) : BASE;
+};
 
 // a += w v on 4 slices, as two packed fma.rn.f32x2 (sm_100: two lanes of
 // round-to-nearest FMA per instruction, the same results as four fmaf; half
@@ -402,7 +414,7 @@ inline cudaError_t dd_allow_dyn(K kernel, int bytes) {
 
 // One CTA per (view row, channel block, z-tile group) of one call.
 template <int ZL, int CG, int NZ>
-__global__ void __launch_bounds__(256, DDFAN_DD_FWD_MIN_CTAS) k_fwd_dd(const __grid_constant__ DdFwdArgs a) {
+__global__ void __launch_bounds__(256, (DdMinCtas<NZ, DDFAN_DD_FWD_MIN_CTAS>::v)) k_fwd_dd(const __grid_constant__ DdFwdArgs a) {
 #if DDFAN_DD_FWD_ROWS_X
   fwd_dd_body<ZL, CG, NZ>(a, a.row0 + (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z);
 #else
@@ -413,7 +425,7 @@ __global__ void __launch_bounds__(256, DDFAN_DD_FWD_MIN_CTAS) k_fwd_dd(const __g
 // One launch over a work list of many calls (batched reconstructions): CTA
 // b takes item {call, view row, channel block, z-tile group} = items[b].
 template <int ZL, int CG, int NZ>
-__global__ void __launch_bounds__(256, DDFAN_DD_FWD_MIN_CTAS) k_fwd_dd_batch(const DdFwdArgs* __restrict__ args,
+__global__ void __launch_bounds__(256, (DdMinCtas<NZ, DDFAN_DD_FWD_MIN_CTAS>::v)) k_fwd_dd_batch(const DdFwdArgs* __restrict__ args,
                                                                               const int4* __restrict__ items) {
   const int4 it = items[blockIdx.x];
   const DdFwdArgs a = args[it.x];  // a local copy: its fields stay in registers
@@ -600,13 +612,13 @@ __device__ __forceinline__ void back_dd_body(const DdAdjArgs& a, int tile, int z
 
 // One CTA per (voxel tile, z-tile group) of one call.
 template <int ZL, bool XM, int NZ>
-__global__ void __launch_bounds__(256, DDFAN_DD_BACK_MIN_CTAS) k_back_dd(const __grid_constant__ DdAdjArgs a) {
+__global__ void __launch_bounds__(256, (DdMinCtas<NZ, DDFAN_DD_BACK_MIN_CTAS>::v)) k_back_dd(const __grid_constant__ DdAdjArgs a) {
   back_dd_body<ZL, XM, NZ>(a, (int)blockIdx.x, (int)blockIdx.z);
 }
 
 // The work-list launch: CTA b takes item {call, voxel tile, z-tile group} = items[b].
 template <int ZL, bool XM, int NZ>
-__global__ void __launch_bounds__(256, DDFAN_DD_BACK_MIN_CTAS) k_back_dd_batch(const DdAdjArgs* __restrict__ args,
+__global__ void __launch_bounds__(256, (DdMinCtas<NZ, DDFAN_DD_BACK_MIN_CTAS>::v)) k_back_dd_batch(const DdAdjArgs* __restrict__ args,
                                                                                 const int4* __restrict__ items) {
   const int4 it = items[blockIdx.x];
   const DdAdjArgs a = args[it.x];  // a local copy: its fields stay in registers
@@ -732,13 +744,13 @@ __device__ __forceinline__ void ref_dd_body(const DdRefArgs& a, int tile, int zg
 
 // One CTA per (voxel tile, z-tile group) of one call.
 template <int ZL, int NZ>
-__global__ void __launch_bounds__(256, DDFAN_DD_BACK_MIN_CTAS) k_back_ref_dd(const __grid_constant__ DdRefArgs a) {
+__global__ void __launch_bounds__(256, (DdMinCtas<NZ, DDFAN_DD_BACK_MIN_CTAS>::v)) k_back_ref_dd(const __grid_constant__ DdRefArgs a) {
   ref_dd_body<ZL, NZ>(a, (int)blockIdx.x, (int)blockIdx.z);
 }
 
 // The work-list launch: CTA b takes item {call, voxel tile, z-tile group} = items[b].
 template <int ZL, int NZ>
-__global__ void __launch_bounds__(256, DDFAN_DD_BACK_MIN_CTAS) k_back_ref_dd_batch(const DdRefArgs* __restrict__ args,
+__global__ void __launch_bounds__(256, (DdMinCtas<NZ, DDFAN_DD_BACK_MIN_CTAS>::v)) k_back_ref_dd_batch(const DdRefArgs* __restrict__ args,
                                                                                     const int4* __restrict__ items) {
   const int4 it = items[blockIdx.x];
   const DdRefArgs a = args[it.x];  // a local copy: its fields stay in registers
