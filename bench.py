@@ -830,9 +830,12 @@ def run_ours(args):
         line["plain_fp32"] = plain_fp32_iteration(s, (x0, y0, xds, yds), y, mask)
 
     # ---- the same iteration in the other modes (compensated tables, the exact adjoint)
-    if not args.no_modes and rank == 0 and args.views == "shared":
+    if not args.no_modes and rank == 0:
         modes = {}
-        for sat, back in (("hilo", "ref"), ("hilo", "adj"), ("direct", "adj"), ("direct", "ref")):
+        # per-slice lists run on the tables in every mode: only the backprojector varies
+        pairs = (("hilo", "ref"), ("hilo", "adj"), ("direct", "adj"), ("direct", "ref")) if args.views == "shared" \
+            else ((args.sat, "adj"), (args.sat, "ref"))
+        for sat, back in pairs:
             if (sat, back) != (args.sat, args.back):
                 modes["%s/%s" % (sat, back)] = mode_rate(s, (x0, y0, xds, yds), y, mask, hangs, sat, back, local)
         line["other_modes"] = {"iters_per_s": modes,

@@ -11,7 +11,7 @@ pytestmark = pytest.mark.gpu
 # (side, slices, views, subsets, masked, FISTA, non-negativity, backprojector)
 CASES = [(48, 5, 96, 4, True, 1, 1, "adj"), (40, 12, 72, 6, False, 1, 0, "adj"),
          (64, 8, 120, 5, True, 0, 1, "ref"), (32, 33, 90, 3, False, 1, 1, "adj"),
-         (56, 17, 60, 4, True, 1, 0, "ref")]
+         (56, 17, 60, 4, True, 1, 0, "ref"), (24, 100, 36, 3, True, 1, 1, "ref")]
 
 
 def _case(configs, dd2, O, N, Z, P, nsub, masked, seed):
