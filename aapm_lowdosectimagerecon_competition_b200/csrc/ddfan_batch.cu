@@ -17,6 +17,7 @@
 // reconstruction per MATLAB call (AAPM_script/OSSART_AAPM.m:85, :92).
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 #include <map>
 #include <memory>
 #include <tuple>
@@ -38,6 +39,7 @@ enum BatchKind { BK_FWD = 0, BK_ADJ_X = 1, BK_ADJ_Y = 2, BK_REF = 3 };
 struct BatchLaunch {
   int kind, ZL, NZ;
   size_t items_off, nitems;
+  int group;  // the solver group whose chain the launch belongs to
 };
 
 int fwd_cw(int ZL, int NZ) {
@@ -84,6 +86,12 @@ void go_ref(const DdRefArgs* a, const int4* it, unsigned n, cudaStream_t st) {
   k_back_ref_dd_batch<ZL, NZ><<<n, 256, 0, st>>>(a, it);
 }
 
+// solver groups whose launch chains run side by side (DDFAN_BATCH_GROUPS in
+// the environment overrides it)
+#ifndef DDFAN_BATCH_GROUPS
+#define DDFAN_BATCH_GROUPS 1
+#endif
+
 // the work-list forward kernels' dynamic shared memory on the current device
 // (at every batch creation: the attribute belongs to the context)
 int batch_prepare_device(int dev) {
@@ -125,6 +133,12 @@ struct Batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   int kernel_launches = 0;
+  // side streams and events of the solver groups' chains (parallel branches
+  // of the captured graph); group g's launches are contiguous in `launches`
+  int groups = 1;
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> join;
+  cudaEvent_t fork = nullptr;
 };
 
 static void batch_free(Batch* b) {
@@ -142,14 +156,17 @@ static void batch_free(Batch* b) {
   for (void* q : ptrs) dev_free(q, b->own);
   if (b->own) cudaStreamDestroy(b->own);
   if (b->last_use) cudaEventDestroy(b->last_use);
+  for (cudaStream_t q : b->side) cudaStreamDestroy(q);
+  for (cudaEvent_t q : b->join) cudaEventDestroy(q);
+  if (b->fork) cudaEventDestroy(b->fork);
   cudaGetLastError();
   if (prev >= 0) cudaSetDevice(prev);
   delete b;
 }
 
-// The launches of one batched iteration (every solve's next iteration).
-static int batch_iteration(Batch& b, cudaStream_t st) {
-  for (const BatchLaunch& L : b.launches) {
+// One launch of the work list on st.
+static int batch_launch(Batch& b, const BatchLaunch& L, cudaStream_t st) {
+  {
     const int4* it = b.d_items + L.items_off;
     const unsigned n = (unsigned)L.nitems;
     if (L.kind == BK_FWD) {
@@ -205,6 +222,35 @@ static int batch_iteration(Batch& b, cudaStream_t st) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "batched launch (kind %d): %s", L.kind, cudaGetErrorString(e));
   }
+  return DDFAN_OK;
+}
+
+// The launches of one batched iteration (every solve's next iteration).  With
+// several solver groups each group's launches form a chain of their own on a
+// side stream forked from st and joined back before FISTA (under capture:
+// parallel branches of the graph), so one group's forward projections run
+// beside another's backprojections, as separate solves on separate streams
+// do; within a group the launches keep the step order.
+static int batch_iteration(Batch& b, cudaStream_t st) {
+  const bool fork = b.groups > 1 && !b.side.empty();
+  cudaError_t e = cudaSuccess;
+  if (fork) {
+    e = cudaEventRecord(b.fork, st);
+    for (size_t t = 0; t < b.side.size() && e == cudaSuccess; ++t) e = cudaStreamWaitEvent(b.side[t], b.fork, 0);
+    if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "batch: fork: %s", cudaGetErrorString(e));
+  }
+  for (const BatchLaunch& L : b.launches) {
+    const cudaStream_t q = fork && L.group > 0 ? b.side[L.group - 1] : st;
+    const int rc = batch_launch(b, L, q);
+    if (rc) return rc;
+  }
+  if (fork) {
+    for (size_t t = 0; t < b.side.size() && e == cudaSuccess; ++t) {
+      e = cudaEventRecord(b.join[t], b.side[t]);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(st, b.join[t], 0);
+    }
+    if (e != cudaSuccess) return set_err(DDFAN_ERR_CUDA, "batch: join: %s", cudaGetErrorString(e));
+  }
   if (b.nfista) {
     ProfScope ps(KIND_FISTA, st);
     const int blocks = (int)std::max<size_t>(1, std::min<size_t>((b.fista_max + 255) / 256, 1024));
@@ -245,11 +291,26 @@ static int batch_create(Batch** out, Solver* const* solvers, int n) {
   std::vector<DdAdjArgs> aargs;
   std::vector<DdRefArgs> rargs;
   std::vector<int4> items;
-  // per step: class -> items, for each kind
+  // solver groups: largest solves first, dealt round robin
+  int G = DDFAN_BATCH_GROUPS;
+  if (const char* v = getenv("DDFAN_BATCH_GROUPS")) G = atoi(v);
+  G = std::max(1, std::min(G, (int)b.sv.size()));
+  b.groups = G;
+  std::vector<int> group_of(b.sv.size());
+  {
+    std::vector<int> order(b.sv.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+    auto work = [&](int i) { const Solver& s = *b.sv[i]; return (double)s.XN * s.YN * s.Zi * s.PNall; };
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return work(x) > work(y); });
+    for (size_t r = 0; r < order.size(); ++r) group_of[order[r]] = (int)(r % G);
+  }
+  // per group, per step: class -> items, for each kind
+  for (int grp = 0; grp < G; ++grp)
   for (int k = 0; k < maxsub; ++k) {
     std::map<std::pair<int, int>, std::vector<int4>> fwd, adjx, adjy, ref;
-    for (Solver* sp : b.sv) {
-      Solver& s = *sp;
+    for (size_t si = 0; si < b.sv.size(); ++si) {
+      if (group_of[si] != grp) continue;
+      Solver& s = *b.sv[si];
       if (k >= s.nsub) continue;
       const Plan& p = *s.P;
       const int o = s.off[k], c = s.cnt[k];
@@ -319,7 +380,7 @@ static int batch_create(Batch** out, Solver* const* solvers, int n) {
     auto emit = [&](int kind, std::map<std::pair<int, int>, std::vector<int4>>& m) {
       for (auto& kv : m) {
         if (kv.second.empty()) continue;
-        BatchLaunch L{kind, kv.first.first, kv.first.second, items.size(), kv.second.size()};
+        BatchLaunch L{kind, kv.first.first, kv.first.second, items.size(), kv.second.size(), grp};
         items.insert(items.end(), kv.second.begin(), kv.second.end());
         b.launches.push_back(L);
       }
@@ -342,6 +403,17 @@ static int batch_create(Batch** out, Solver* const* solvers, int n) {
   b.kernel_launches = (int)b.launches.size() + (b.nfista ? 2 : 0);
   cudaError_t e = cudaStreamCreateWithFlags(&b.own, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b.last_use, cudaEventDisableTiming);
+  if (b.groups > 1) {
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b.fork, cudaEventDisableTiming);
+    for (int t = 1; t < b.groups && e == cudaSuccess; ++t) {
+      cudaStream_t q = nullptr;
+      cudaEvent_t ev = nullptr;
+      e = cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking);
+      if (e == cudaSuccess) b.side.push_back(q);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+      if (e == cudaSuccess) b.join.push_back(ev);
+    }
+  }
   if (e != cudaSuccess) {
     cudaGetLastError();
     return set_err(DDFAN_ERR_CUDA, "batch: stream/event creation: %s", cudaGetErrorString(e));
