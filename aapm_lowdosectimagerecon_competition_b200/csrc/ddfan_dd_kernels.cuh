@@ -667,9 +667,9 @@ __device__ __forceinline__ void ref_dd_body(const DdRefArgs& a, int tile, int zg
   constexpr int NT = T::NT, VG = T::VG, SPL = T::SPL, KT = T::KT, LT = T::LT;
   constexpr int NW = NT / 32, GW = 32 / ZL;
   constexpr int VCW = ZL;  // views per warp chunk
-  __shared__ int2 s_i[NW][VCW][GW][VG];
-  __shared__ float2 s_f[NW][VCW][GW][VG];
-  __shared__ float s_w[NW][VCW][GW][VG];
+  // per (view, voxel): the walk's weights (w0, wm, we) and both channel cells
+  // packed (k0 | k1 << 16), decoded once here for the ZL z-lanes that walk it
+  __shared__ float4 s_g[NW][VCW][GW][VG];
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
   const int zl = lane % ZL, gw = lane / ZL;
   const int zt_first = a.zt0 + zgrp * NZ;
@@ -724,9 +724,8 @@ __device__ __forceinline__ void ref_dd_body(const DdRefArgs& a, int tile, int zg
         ii = make_int2(min((int)cL, a.U - 1), min((int)cR, a.U - 1));
         ff = make_float2((float)(cL - ii.x), (float)(cR - ii.y));
       }
-      s_i[w][vv][gl][v] = ii;
-      s_f[w][vv][gl][v] = ff;
-      s_w[w][vv][gl][v] = wt;
+      const float3 ww = walk3(ii.x, ff.x, ii.y, ff.y, wt);
+      s_g[w][vv][gl][v] = make_float4(ww.x, ww.y, ww.z, __int_as_float(pack_k(ii.x, ii.y)));
     }
     __syncwarp();
     if (active) {
@@ -734,14 +733,13 @@ __device__ __forceinline__ void ref_dd_body(const DdRefArgs& a, int tile, int zg
         const float4* base = a.q + (size_t)(v0 + vv) * vstride + zbk[0];
 #pragma unroll
         for (int v = 0; v < VG; ++v) {
-          const int2 ii = s_i[w][vv][gw][v];
-          const float2 ff = s_f[w][vv][gw][v];
-          const float3 wt = walk3(ii.x, ff.x, ii.y, ff.y, s_w[w][vv][gw][v]);
+          const float4 g = s_g[w][vv][gw][v];
+          const int pk = __float_as_int(g.w), k0 = pk & 0xffff, k1 = pk >> 16;
           float4 cur[NZ];
-          const float4* p0 = base + (size_t)ii.x * P4;
+          const float4* p0 = base + (size_t)k0 * P4;
 #pragma unroll
           for (int z = 0; z < NZ; ++z) cur[z] = __ldg(p0 + zoff[z]);
-          walk_nz<NZ>(acc[v], cur, vm, base, P4, zoff, ii.x, ii.y, a.U, make_float4(wt.x, wt.y, wt.z, 0.f));
+          walk_nz<NZ>(acc[v], cur, vm, base, P4, zoff, k0, k1, a.U, g);
         }
       }
     }
