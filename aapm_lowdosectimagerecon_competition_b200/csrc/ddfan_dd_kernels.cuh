@@ -498,6 +498,9 @@ __device__ __forceinline__ void back_dd_body(const DdAdjArgs& a, int tile, int z
   constexpr int NEG = VG + 1;                // edges per group
   constexpr int TBMAX = 1024, LUTMAX = 4096;
   __shared__ int2 s_geo[NW][VCW][GW][NEG];
+  // per (view, pixel): the walk's weights and both edge cells packed, decoded
+  // once for the ZL z-lanes that walk it
+  __shared__ float4 s_wk[NW][VCW][GW][VG];
   __shared__ int s_p[NW][VCW];
   __shared__ float s_sgn[NW][VCW];
   __shared__ float s_tb[TBMAX];
@@ -582,29 +585,31 @@ __device__ __forceinline__ void back_dd_body(const DdAdjArgs& a, int tile, int z
       s_geo[w][vv][gl][ke] = make_int2(b, __float_as_int(frac));
     }
     __syncwarp();
+    // the walk of pixel v runs from edge v to edge v + 1 (chained: its end is
+    // the next pixel's start)
+    for (int e = lane; e < VCW * GW * VG; e += 32) {
+      const int vv = e / (GW * VG), r = e - vv * (GW * VG);
+      const int gl = r / VG, v = r - gl * VG;
+      const int2 g0 = s_geo[w][vv][gl][v], g1 = s_geo[w][vv][gl][v + 1];
+      const float3 ww = walk3(g0.x, __int_as_float(g0.y), g1.x, __int_as_float(g1.y), s_sgn[w][vv]);
+      s_wk[w][vv][gl][v] = make_float4(ww.x, ww.y, ww.z, __int_as_float(pack_k(g0.x, g1.x)));
+    }
+    __syncwarp();
     if (active) {
       for (int vv = 0; vv < nvc; ++vv) {
         const float4* base = a.w + (size_t)s_p[w][vv] * vstride + zbk[0];
-        const float sgn = s_sgn[w][vv];
-        const int2* geo = &s_geo[w][vv][gw][0];
-        int2 gi = geo[0];
-        int k = gi.x;
-        float f = __int_as_float(gi.y);
+        const float4* wk = &s_wk[w][vv][gw][0];
         float4 cur[NZ];
         {
-          const float4* p0 = base + (size_t)k * P4;
+          const float4* p0 = base + (size_t)(__float_as_int(wk[0].w) & 0xffff) * P4;
 #pragma unroll
           for (int z = 0; z < NZ; ++z) cur[z] = __ldg(p0 + zoff[z]);
         }
 #pragma unroll
         for (int v = 0; v < VG; ++v) {
-          gi = geo[v + 1];
-          const int k1 = gi.x;
-          const float f1 = __int_as_float(gi.y);
-          const float3 wt = walk3(k, f, k1, f1, sgn);
-          walk_nz<NZ>(acc[v], cur, vm, base, P4, zoff, k, k1, a.U, make_float4(wt.x, wt.y, wt.z, 0.f));
-          k = k1;
-          f = f1;
+          const float4 g = wk[v];
+          const int pk = __float_as_int(g.w);
+          walk_nz<NZ>(acc[v], cur, vm, base, P4, zoff, pk & 0xffff, pk >> 16, a.U, g);
         }
       }
     }
