@@ -93,7 +93,7 @@ int ps_back_ref(int mode, const PsBackArgs& a, int Z, cudaStream_t st) {
   mode = cell_mode(mode);  // these tables keep hi/lo cells in the direct mode
   if (Z < 1) return DDFAN_OK;
   if (Z > 65535) return set_err(DDFAN_ERR_UNSUPPORTED, "slice-major backprojection: %d slices", Z);
-  dim3 grid((a.XN + 63) / 64, (a.YN + 4 * kPsBackRows - 1) / (4 * kPsBackRows), Z);
+  dim3 grid((a.XN + 63) / 64, (a.YN + 4 * kPsRefRows - 1) / (4 * kPsRefRows), Z);
   ProfScope ps(KIND_BACK_A, st);
   switch (mode) {
     case SAT_FP32: k_ps_back_ref<SAT_FP32><<<grid, 256, 0, st>>>(a); break;

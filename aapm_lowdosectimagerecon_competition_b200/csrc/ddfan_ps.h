@@ -65,6 +65,11 @@ struct PsBackArgs {
 
 // rows of pixels per warp in k_ps_back_adj (8 warps: 2 across x, 4 down y)
 constexpr int kPsBackRows = 8;
+// and in k_ps_back_ref, whose full FP64 angle is taken on a warp's first row
+#ifndef DDFAN_PS_REF_ROWS
+#define DDFAN_PS_REF_ROWS 8
+#endif
+constexpr int kPsRefRows = DDFAN_PS_REF_ROWS;
 
 // out[b][c][r] = in[b][r][c] for b < B, r < R, c < C
 int ps_transpose(const float* in, float* out, int B, long long R, int C, cudaStream_t st);

@@ -529,7 +529,7 @@ __global__ void __launch_bounds__(256) k_ps_back_adj(PsBackArgs a) {
 // k_ps_back_adj, with k_back_ref's mask rule (masked voxels get 0).
 template <int M>
 __global__ void __launch_bounds__(256) k_ps_back_ref(PsBackArgs a) {
-  constexpr int R = kPsBackRows, PX = 32;
+  constexpr int R = kPsRefRows, PX = 32;
   using Cell = typename PsCell<M>::T;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int z = blockIdx.z;
