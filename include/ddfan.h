@@ -171,8 +171,9 @@ DDFAN_API int ddfan_back_dev(ddfan_plan* plan, const float* d_angs, int PN, int 
  * that every GPU loading this library holds until exit; a problem needing more
  * returns DDFAN_ERR_UNSUPPORTED before any GPU work.  The first call on a device
  * -- and the first after a cudaDeviceReset, which gives the device a new
- * context -- looks up that array's device address (cudaGetSymbolAddress);
- * make that first call before any stream capture.  A call made while its
+ * context -- looks up that array's device address (cudaGetSymbolAddress) and
+ * allows the direct-mode forward kernels their shared memory
+ * (cudaFuncSetAttribute); make that first call before any stream capture.  A call made while its
  * stream is being captured returns DDFAN_ERR_UNSUPPORTED: every call uploads
  * its geometry from host memory that is gone when it returns.  Calls share
  * the array, so calls whose kernels overlap on one GPU race: serialise them
