@@ -207,6 +207,10 @@ struct DdFwdArgs {
 #ifndef DDFAN_DD_FWD_PART
 #define DDFAN_DD_FWD_PART 2
 #endif
+// geometry chunks per ray-sum chunk (DDFAN_DD_FWD_PART == 2)
+#ifndef DDFAN_DD_FWD_FLUSH
+#define DDFAN_DD_FWD_FLUSH 1
+#endif
 // most z-tiles per thread (1, 2 or 4; fewer when a call has fewer)
 #ifndef DDFAN_DD_NZ
 #define DDFAN_DD_NZ 4
@@ -345,16 +349,18 @@ __device__ __forceinline__ void fwd_dd_body(const DdFwdArgs& a, int row, int cbl
 #pragma unroll
           for (int s = 0; s < 4; ++s) acc[j][z][s] += part[j][z][s];
 #elif DDFAN_DD_FWD_PART == 2
+      if ((ii0 / CC) % DDFAN_DD_FWD_FLUSH == DDFAN_DD_FWD_FLUSH - 1 || ii0 + CC >= nl) {
 #pragma unroll
-      for (int j = 0; j < CG; ++j)
+        for (int j = 0; j < CG; ++j)
 #pragma unroll
-        for (int z = 0; z < NZ; ++z)
+          for (int z = 0; z < NZ; ++z)
 #pragma unroll
-          for (int s = 0; s < 4; ++s) {
-            float* t = tot + ((j * NZ + z) * 4 + s) * T::NT;
-            *t += acc[j][z][s];
-            acc[j][z][s] = 0.f;
-          }
+            for (int s = 0; s < 4; ++s) {
+              float* t = tot + ((j * NZ + z) * 4 + s) * T::NT;
+              *t += acc[j][z][s];
+              acc[j][z][s] = 0.f;
+            }
+      }
 #endif
     }
     __syncwarp();
