@@ -25,7 +25,10 @@ def _case(configs, dd2, O, N, Z, P, nsub, masked, seed):
     return s, (x0, y0, xds, yds), mask, y
 
 
-def test_batched_solves_equal_solo_solves_and_oracle():
+@pytest.mark.parametrize("groups", ["1", "3"])
+def test_batched_solves_equal_solo_solves_and_oracle(monkeypatch, groups):
+    # groups > 1: the solves' launch chains run side by side (graph branches)
+    monkeypatch.setenv("DDFAN_BATCH_GROUPS", groups)
     import torch
     from aapm_lowdosectimagerecon_competition_b200 import configs, dd2, device
     from oracle import oracle as O
